@@ -1,0 +1,293 @@
+/*
+ * pourlab.h — C ABI of the B200 pour-substep engine (libpourlab_cuda.so).
+ *
+ * The engine simulates the 3D teapot pour of PourLab's src/sim3d solver: a half pot behind a
+ * symmetry plane, FLIP/PIC parcels on a staggered MAC grid, two pressure-type solves per substep,
+ * a target-volume pour controller, and per-layer accounting of the poured volume. Every entry
+ * point below replaces one member of the reference's TypeScript surface; the citation after each
+ * declaration names it (paths inside marcelpetrick/teapotFluidSimulation).
+ *
+ * Conventions
+ *   - Status codes: 0 = ok, negative = error (PL_E_*). pl_last_error() returns a message for the
+ *     last failing call on the calling thread. Non-convergence of a pressure solve is not an error:
+ *     it is counted in pl_diagnostics.pressure_failures, as the reference counts it.
+ *   - Ownership: a pl_sim owns all of its device memory; the caller owns every output buffer.
+ *   - Threading: one handle per host thread. Calls are synchronous and not reentrant. Each handle
+ *     runs on its own CUDA stream on the device that was current when it was created.
+ *   - Units: SI (metres, seconds, m^3), angles in degrees where the name says deg.
+ */
+#ifndef POURLAB_H
+#define POURLAB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PL_OK 0
+#define PL_E_ARG (-1)      /* invalid argument or size */
+#define PL_E_CUDA (-2)     /* a CUDA call failed (message names it) */
+#define PL_E_TIMEOUT (-3)  /* a bounded device-side wait gave up */
+#define PL_E_STATE (-4)    /* call not valid in the current state */
+#define PL_E_NOMEM (-5)    /* device or host allocation failed */
+#define PL_NONE 1          /* query has no value yet (e.g. fractions before any pour) */
+
+/* Cell types (solver3d.ts:17-19) and parcel status (solver3d.ts:20-23). */
+#define PL_AIR 0
+#define PL_FLUID 1
+#define PL_SOLID 2
+#define PL_IN_POT 0
+#define PL_DISCHARGED 1
+#define PL_SPILLED 2
+#define PL_LOST 3
+
+/* Motion kinds and controller phases (src/sim/types.ts:57, src/sim/motion.ts:9). */
+enum pl_motion_kind { PL_MOTION_STILL = 0, PL_MOTION_POUR = 1, PL_MOTION_TILT = 2, PL_MOTION_MANUAL = 3 };
+enum pl_phase {
+  PL_PHASE_WAIT = 0,
+  PL_PHASE_TILT_IN = 1,
+  PL_PHASE_HOLD = 2,
+  PL_PHASE_RETURN = 3,
+  PL_PHASE_REST = 4,
+  PL_PHASE_DONE = 5,
+  PL_PHASE_MANUAL = 6
+};
+
+/* Pressure preconditioner. MIC0 is the reference's MIC(0) (solver3d.ts:883-900, 955-973),
+ * applied in wavefront order on the device; MG is a 3D geometric multigrid V-cycle (the 3D form
+ * of src/sim/multigrid.ts with a red-black Gauss-Seidel smoother). */
+enum pl_preconditioner { PL_PRECOND_MIC0 = 0, PL_PRECOND_MG = 1 };
+/* Arithmetic of the pressure solves: F64 keeps every solver vector in FP64; MIXED keeps the
+ * Krylov and smoother vectors in FP32 with FP64 inner products, an FP64 solution and FP64
+ * iterative refinement of the true residual. */
+enum pl_solve_precision { PL_SOLVE_F64 = 0, PL_SOLVE_MIXED = 1 };
+
+/* Teapot3DConfig (src/sim3d/vessel3d.ts:9-20). */
+typedef struct pl_teapot {
+  double radius;          /* inner radius of the body (m) */
+  double height;          /* inner height of the body (m) */
+  double wall;            /* wall thickness (m) */
+  double inlet_height;    /* spout inlet centre height (m) */
+  double bore_radius;     /* spout bore radius (m) */
+  double spout_angle_deg; /* spout elevation (deg) */
+  double spout_length;    /* spout length (m) */
+} pl_teapot;
+
+/* MotionConfig (src/sim/types.ts:55-84). */
+typedef struct pl_motion {
+  int32_t kind; /* enum pl_motion_kind */
+  int32_t repeats;
+  double start_delay;
+  double tilt_duration;
+  double hold_angle_deg;
+  double hold_tilt_rate;
+  double max_angle_deg;
+  double return_duration;
+  double max_hold;
+  double hold_time;
+  double target_volume; /* m^3 */
+  double anticipation;
+  double repeat_gap;
+  double settle_time;
+} pl_motion;
+
+/* Config3D (src/sim3d/solver3d.ts:25-43) plus the engine's own settings at the end. */
+typedef struct pl_config {
+  pl_teapot teapot;
+  double h;              /* cell size (m) */
+  double initial_volume; /* liquid volume of the whole pot (m^3) */
+  pl_motion motion;
+  double pivot[2]; /* tilt pivot in pot-local x, y (m) */
+  double gravity;
+  double flip_ratio;
+  double density_correction;
+  double cfl;
+  double max_substep;
+  double pressure_tolerance;
+  int32_t pressure_max_iterations;
+  uint32_t seed;
+  double duration;
+  /* engine settings (no counterpart in Config3D) */
+  int32_t preconditioner;  /* enum pl_preconditioner */
+  int32_t solve_precision; /* enum pl_solve_precision */
+  int32_t reserved[6];
+} pl_config;
+
+/* Diagnostics3D (src/sim3d/solver3d.ts:45-60). */
+typedef struct pl_diagnostics {
+  double time;
+  int64_t steps;
+  double angle_deg;
+  int32_t phase; /* enum pl_phase */
+  int32_t particles;
+  int32_t grid[3];
+  int32_t pressure_iterations;   /* iterations of the last pressure solve */
+  int32_t pressure_failures;     /* pressure solves that hit the iteration cap */
+  int32_t correction_iterations; /* iterations of the last density-correction solve */
+  double discharged_ml;
+  double spilled_ml;
+  double lost_ml;
+  double in_pot_ml;
+  double max_divergence; /* 1/s, after projection */
+  double interior_density;
+} pl_diagnostics;
+
+/* Constructor-derived sizes (solver3d.ts:62-84, 116-228). */
+typedef struct pl_sizes {
+  int32_t n;  /* parcels in the simulated half */
+  int32_t nx, ny, nz;
+  double h;
+  double parcel_volume; /* m^3 per parcel (half-pot volume / n) */
+  double pivot_world[2];
+  double fill_height;
+  int32_t band_counts[3]; /* parcels per origin layer (bottom, middle, top) */
+  int32_t reserved;
+} pl_sizes;
+
+/* PourController internal state (src/sim/motion.ts:21-38): enough to resume a run exactly. */
+typedef struct pl_controller_state {
+  int32_t phase; /* enum pl_phase */
+  int32_t pour;
+  double angle; /* rad */
+  double phase_start;
+  double start_angle;
+  double start_rate;
+  double last_rate;
+  double flow_rate;
+  double last_discharged;
+  double target; /* rad, manual mode */
+  double manual_rate;
+} pl_controller_state;
+
+/* Whole-simulation scalar state beside the parcel arrays (solver3d.ts:86-114). */
+typedef struct pl_sim_state {
+  double time;
+  int64_t steps;
+  double phi;   /* current pose angle (rad, = -tilt) */
+  double omega; /* angular velocity of the last substep (rad/s) */
+  int32_t counts[4];          /* parcels per status */
+  int32_t discharged_by_origin[3];
+  int32_t last_iterations;
+  int32_t failures;
+  int32_t reserved;
+  double max_div;
+  double interior;
+  pl_controller_state controller;
+} pl_sim_state;
+
+/* Field selectors for pl_get_field (face fields are stored u, then v, then w). */
+enum pl_field {
+  PL_FIELD_CELL = 0,     /* u8[nx*ny*nz]: AIR/FLUID/SOLID of the last substep */
+  PL_FIELD_VELOCITY = 1, /* f64[nu+nv+nw]: face velocity after projection and extrapolation */
+  PL_FIELD_VELOCITY_PREV = 2, /* f64[nu+nv+nw]: particle-to-grid result (FLIP reference) */
+  PL_FIELD_PRESSURE = 3,  /* f64[nx*ny*nz]: pressure of the last projection */
+  PL_FIELD_CORRECTION = 4, /* f64[nu+nv+nw]: density-correction face velocity */
+  PL_FIELD_VALID = 5,      /* u8[nu+nv+nw]: face valid mask before extrapolation */
+  PL_FIELD_DENSITY = 6,    /* f64[nx*ny*nz]: particle density (sum of weights) */
+  PL_FIELD_RHS = 7         /* f64[nx*ny*nz]: right-hand side of the last density solve */
+};
+
+/* ------------------------------------------------------------------ presets */
+
+/* defaultTeapot3D() (src/sim3d/vessel3d.ts:22-32). */
+void pl_default_teapot(pl_teapot* out);
+/* defaultMotion() with maxHold 20 (src/sim/config.ts:168-186, src/sim3d/presets3d.ts:17). */
+void pl_default_motion(pl_motion* out);
+/* gentlePour3D(cellMm, seconds) (src/sim3d/presets3d.ts:9-26). */
+void pl_gentle_pour(double cell_mm, double seconds, pl_config* out);
+
+/* ------------------------------------------------------------------ lifetime */
+
+typedef struct pl_sim pl_sim;
+
+/* new Simulation3D(cfg) / new GpuSimulation3D(device, cfg)
+ * (src/sim3d/solver3d.ts:116-228, src/gpu3d/solver.ts:108-124). Seeding, banding and grid sizing
+ * run on the host in FP64 exactly as the reference constructor; the state then moves to the GPU. */
+int pl_create(const pl_config* cfg, pl_sim** out);
+/* GpuSimulation3D.destroy() (src/gpu3d/solver.ts:486-489). Accepts NULL. */
+void pl_destroy(pl_sim* sim);
+/* Message of the last failing call on this thread ("" if none). */
+const char* pl_last_error(void);
+
+/* ------------------------------------------------------------------ queries */
+
+/* n, nx, ny, nz, h, parcelVolume, pivotWorld, fillHeight, bandCounts (solver3d.ts:62-84). */
+int pl_get_sizes(const pl_sim* sim, pl_sizes* out);
+/* stableDt() (solver3d.ts:268-278; src/gpu3d/solver.ts:256-263). Reads the device's max speed. */
+int pl_stable_dt(pl_sim* sim, double* out);
+/* get finished (solver3d.ts:264-266). */
+int pl_finished(const pl_sim* sim);
+
+/* ------------------------------------------------------------------ stepping */
+
+/* step(dt) (solver3d.ts:288-309; src/gpu3d/solver.ts:304-370). dt <= 0 selects
+ * min(stableDt(), duration - time), the default of GpuSimulation3D.step. Synchronous: the
+ * controller and counters are current when it returns. */
+int pl_step(pl_sim* sim, double dt);
+/* advance(duration) (solver3d.ts:281-286; src/gpu3d/solver.ts:373-378): whole stable substeps
+ * until duration has elapsed or the run is finished. The substep sequence runs on the device
+ * (controller, stable dt and counters included) with no host round trip per substep.
+ * out may be NULL. */
+int pl_advance(pl_sim* sim, double duration, pl_diagnostics* out);
+/* Wait for queued device work (GpuSimulation3D.sync, src/gpu3d/solver.ts:289-294). */
+int pl_sync(pl_sim* sim);
+
+/* ------------------------------------------------------------------ controller */
+
+/* controller.setTarget(angleDeg, time) (src/sim/motion.ts:40-44; used at
+ * src/view3d/live.ts:262). Switches nothing by itself: the motion kind must be manual. */
+int pl_set_tilt_target(pl_sim* sim, double angle_deg, double time);
+/* controller.angleDeg and controller.phase (src/sim/motion.ts:156-158, 23). */
+int pl_controller(const pl_sim* sim, double* angle_deg, int32_t* phase);
+
+/* ------------------------------------------------------------------ results */
+
+/* diagnostics() (solver3d.ts:796-814; src/gpu3d/solver.ts:380-399). */
+int pl_get_diagnostics(pl_sim* sim, pl_diagnostics* out);
+/* dischargedFractions() (solver3d.ts:817-823; src/gpu3d/solver.ts:402-406): shares of the
+ * poured parcels by origin layer. Returns PL_NONE (out untouched) before anything poured. */
+int pl_discharged_fractions(pl_sim* sim, double out[3]);
+/* readParticles() (src/gpu3d/solver.ts:409-428): positions and velocities as xyzw float4
+ * (w = 0) in parcel id order, status as u32. Any pointer may be NULL. */
+int pl_read_particles(pl_sim* sim, float* pos4, float* vel4, uint32_t* status);
+/* Same state in FP64 SoA (the arrays Simulation3D exposes: solver3d.ts:75-82). */
+int pl_read_particles_f64(pl_sim* sim, double* x, double* y, double* z, double* vx, double* vy,
+                          double* vz, uint8_t* status);
+/* Simulation3D.origin (solver3d.ts:81): origin layer 0/1/2 per parcel id. */
+int pl_read_origin(const pl_sim* sim, uint8_t* origin);
+/* readRenderPositions() (src/gpu3d/solver.ts:443-475; kernel src/gpu3d/shaders.ts:786-799):
+ * packed xyz of the simulated half then its mirror image, 6*n floats, written by a device kernel
+ * into a device buffer and copied to xyz6n. */
+int pl_read_render_positions(pl_sim* sim, float* xyz6n);
+
+/* ------------------------------------------------------------------ state (parity harness) */
+
+/* Scalar state and parcel arrays in id order (FP64 SoA as in solver3d.ts:75-82). The engine
+ * stores parcels in FP32, so pl_set_state rounds them. Any parcel pointer may be NULL on get. */
+int pl_get_state(pl_sim* sim, pl_sim_state* st);
+int pl_set_state(pl_sim* sim, const pl_sim_state* st, const double* x, const double* y,
+                 const double* z, const double* vx, const double* vy, const double* vz,
+                 const uint8_t* status);
+/* Copy one grid field of the last substep to host memory (enum pl_field); count is the number of
+ * elements the caller's buffer holds. u8 fields are written as uint8_t, others as double. */
+int pl_get_field(pl_sim* sim, int32_t field, void* out, size_t count);
+
+/* ------------------------------------------------------------------ standalone pressure solve */
+
+/* Pcg3D.solve(cell, b, q, tol, maxIter) (solver3d.ts:858-937) as a standalone call on
+ * caller-provided device buffers: cell u8[nx*ny*nz], b and q f64[nx*ny*nz]. Runs the chosen
+ * preconditioner on stream (0 = legacy default stream) and writes iterations, converged and
+ * the final max-norm residual to host memory after synchronising. Scratch memory is allocated
+ * by the call and freed before it returns. */
+int pl_pcg_solve_device(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny,
+                        int32_t nz, double tol, int32_t max_iter, int32_t preconditioner,
+                        int32_t precision, void* stream, int32_t* iterations, int32_t* converged,
+                        double* residual);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POURLAB_H */

@@ -1,0 +1,632 @@
+// C ABI of the pour engine (include/pourlab.h): construction, the substep graph, stepping and the
+// read-back of parcels, fields and diagnostics.
+//
+// A substep is a fixed sequence of kernels (kernels.cu, solver.cu) captured once into a CUDA graph.
+// All per-substep decisions (stable dt, controller, liquid-cell count, solver convergence) are made
+// on the device, so advance() launches the graph back to back and synchronises only to learn when
+// the requested duration has elapsed; substeps launched past the end return immediately.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "setup.h"
+
+using namespace pl;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) return fail(PL_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct pl_sim {
+  Geo g{};
+  DevPtrs P{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void* mem = nullptr;
+  size_t mem_bytes = 0;
+  SimScalars hs{};  // host mirror, current after every synchronising call
+  double fill_height = 0;
+  int band_counts[3] = {0, 0, 0};
+  std::vector<uint8_t> origin;
+  pl_config cfg{};
+  float* export_buf = nullptr;  // F floats for exported face fields
+};
+
+namespace {
+
+int pull_scalars(pl_sim* s) {
+  CK(cudaMemcpyAsync(&s->hs, s->P.sc, sizeof(SimScalars), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  if (s->hs.errors) {
+    int e = s->hs.errors;
+    return fail(PL_E_TIMEOUT, "device error flags 0x%x (%s%s)", e, (e & ERR_SCAN_TIMEOUT) ? "bin scan wait gave up " : "",
+                (e & ERR_SOLVER_SIZE) ? "solver wavefronts exceed capacity" : "");
+  }
+  return PL_OK;
+}
+
+int push_scalars(pl_sim* s) {
+  CK(cudaMemcpyAsync(s->P.sc, &s->hs, sizeof(SimScalars), cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return PL_OK;
+}
+
+void record_substep(pl_sim* s) {
+  launch_substep_front(s->g, s->P, s->st);
+  launch_pressure_solve(s->g, s->P, s->st);
+  launch_substep_middle(s->g, s->P, s->st);
+  launch_correction_solve(s->g, s->P, s->st);
+  launch_substep_back(s->g, s->P, s->st);
+}
+
+int build_graph(pl_sim* s) {
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+  record_substep(s);
+  CK(cudaStreamEndCapture(s->st, &graph));
+  cudaError_t e = cudaGraphInstantiate(&s->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(PL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  return PL_OK;
+}
+
+double host_stable_dt(const pl_sim* s) {  // solver3d.ts:268-278 on the device's max speed
+  const Geo& g = s->g;
+  double m;
+  std::memcpy(&m, &s->hs.max_speed_bits, 8);
+  double speed = std::sqrt(m) + std::sqrt(5 * g.h * g.gravity) + std::fabs(s->hs.omega) * g.R;
+  return std::min(g.max_substep, (g.cfl * g.h) / speed);
+}
+
+bool host_finished(const pl_sim* s) { return s->hs.time >= s->g.duration - 1e-9; }
+
+// Parcels in id order -> home layout (slot = id).
+int upload_parcels(pl_sim* s, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+                   const double* vz, const uint8_t* status) {
+  const int n = s->g.n;
+  std::vector<float4> pos(n), vel(n);
+  for (int p = 0; p < n; p++) {
+    int st = status ? status[p] : 0;
+    pos[p] = make_float4((float)x[p], (float)y[p], (float)z[p], 0.f);
+    std::memcpy(&pos[p].w, &p, 4);
+    vel[p] = make_float4(vx ? (float)vx[p] : 0.f, vy ? (float)vy[p] : 0.f, vz ? (float)vz[p] : 0.f, 0.f);
+    int meta = st | (int(s->origin[p]) << 8);
+    std::memcpy(&vel[p].w, &meta, 4);
+  }
+  CK(cudaMemcpyAsync(s->P.pos_home, pos.data(), size_t(n) * 16, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->P.vel_home, vel.data(), size_t(n) * 16, cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return PL_OK;
+}
+
+// Home layout -> id order.
+int download_parcels(pl_sim* s, std::vector<float4>& pos, std::vector<float4>& vel) {
+  const int n = s->g.n;
+  std::vector<float4> hp(n), hv(n);
+  CK(cudaMemcpyAsync(hp.data(), s->P.pos_home, size_t(n) * 16, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaMemcpyAsync(hv.data(), s->P.vel_home, size_t(n) * 16, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  pos.resize(n);
+  vel.resize(n);
+  for (int i = 0; i < n; i++) {
+    int id;
+    std::memcpy(&id, &hp[i].w, 4);
+    if (id < 0 || id >= n) return fail(PL_E_STATE, "parcel layout corrupt (id %d at slot %d)", id, i);
+    pos[id] = hp[i];
+    vel[id] = hv[i];
+  }
+  return PL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pl_last_error(void) { return g_err.c_str(); }
+
+void pl_default_teapot(pl_teapot* t) {
+  *t = pl_teapot{0.065, 0.15, 0.008, 0.035, 0.01, 45.0, 0.14};
+}
+
+void pl_default_motion(pl_motion* m) {
+  std::memset(m, 0, sizeof *m);
+  m->kind = PL_MOTION_POUR;
+  m->start_delay = 0.5;
+  m->tilt_duration = 2;
+  m->hold_angle_deg = 22;
+  m->hold_tilt_rate = 3;
+  m->max_angle_deg = 80;
+  m->return_duration = 1.2;
+  m->max_hold = 20;  // gentlePour3D overrides the default 12 (presets3d.ts:17)
+  m->hold_time = 1.5;
+  m->target_volume = 400e-6;
+  m->anticipation = 0.254;
+  m->repeats = 1;
+  m->repeat_gap = 1.5;
+  m->settle_time = 2;
+}
+
+void pl_gentle_pour(double cell_mm, double seconds, pl_config* c) {
+  std::memset(c, 0, sizeof *c);
+  pl_default_teapot(&c->teapot);
+  c->h = cell_mm / 1000;
+  c->initial_volume = 1500 * 1e-6;
+  pl_default_motion(&c->motion);
+  c->pivot[0] = 0;
+  c->pivot[1] = 0.06;
+  c->gravity = 9.81;
+  c->flip_ratio = 0.95;
+  c->density_correction = 0.3;
+  c->cfl = 0.8;
+  c->max_substep = 1.0 / 200;
+  c->pressure_tolerance = 1e-6;
+  c->pressure_max_iterations = 400;
+  c->seed = 1;
+  c->duration = seconds;
+  c->preconditioner = PL_PRECOND_MIC0;
+  c->solve_precision = PL_SOLVE_F64;
+}
+
+int pl_create(const pl_config* cfg, pl_sim** out) {
+  if (!cfg || !out) return fail(PL_E_ARG, "pl_create: null argument");
+  *out = nullptr;
+  char err[256] = "";
+  HostInit init;
+  int rc = host_construct(*cfg, &init, err, sizeof err);
+  if (rc) return fail(rc, "%s", err);
+  pl_sim* s = new pl_sim();
+  s->cfg = *cfg;
+  s->g = init.geo;
+  s->fill_height = init.fill_height;
+  for (int k = 0; k < 3; k++) s->band_counts[k] = init.band_counts[k];
+  s->origin = init.origin;
+  const Geo& g = s->g;
+  cudaGetDevice(&s->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete s;
+    return fail(PL_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  // one allocation for everything
+  const size_t N = g.n, C = g.nc, F = g.nf, B = g.nbins + 1;
+  size_t sizes[] = {
+      N * 16, N * 16, N * 16, N * 16, N * 16, N * 16,  // pos/vel home, pos/vel sorted, frac sorted/tmp
+      N * 4,  N * 4,  N * 8,                           // key, rank, placed
+      B * 4,  B * 4,                                   // cnt, start
+      C,      C * 4,  C * 4,                           // cell, lidx, list
+      C * 8,  C * 8,                                   // q, qc
+      F * 4,  F * 4,  F * 4, F, F,                     // u, uprev, uext, valid, vext
+      C * 8,  C * 8,                                   // rhs, density
+      DENSITY_BLOCKS * 8, DENSITY_BLOCKS * 4,          // interior partials
+      SCAN_MAX_TILES * 8,                              // scan descriptors
+      solver_ws_bytes(int(C)),                         // solver
+      N * 6 * 4,                                       // render
+      sizeof(SimScalars), F * 4,                       // scalars, export
+  };
+  size_t total = 0;
+  for (size_t b : sizes) total += al256(b);
+  e = cudaMalloc(&s->mem, total);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(s->st);
+    delete s;
+    return fail(PL_E_NOMEM, "cudaMalloc(%zu): %s", total, cudaGetErrorString(e));
+  }
+  s->mem_bytes = total;
+  cudaMemsetAsync(s->mem, 0, total, s->st);
+  char* p = static_cast<char*>(s->mem);
+  int idx = 0;
+  auto take = [&]() {
+    char* r = p;
+    p += al256(sizes[idx++]);
+    return (void*)r;
+  };
+  DevPtrs& P = s->P;
+  P.pos_home = (float4*)take();
+  P.vel_home = (float4*)take();
+  P.pos_sorted = (float4*)take();
+  P.vel_sorted = (float4*)take();
+  P.frac_sorted = (float4*)take();
+  P.frac_tmp = (float4*)take();
+  P.key = (int*)take();
+  P.rank = (int*)take();
+  P.placed = (int2*)take();
+  P.cnt = (int*)take();
+  P.start = (int*)take();
+  P.cell = (uint8_t*)take();
+  P.lidx = (int*)take();
+  P.list = (int*)take();
+  P.q = (double*)take();
+  P.qc = (double*)take();
+  P.u = (float*)take();
+  P.uprev = (float*)take();
+  P.uext = (float*)take();
+  P.valid = (uint8_t*)take();
+  P.vext = (uint8_t*)take();
+  P.rhs = (double*)take();
+  P.density = (double*)take();
+  P.interior_part = (double*)take();
+  P.interior_cnt_part = (int*)take();
+  P.scan_state = (unsigned long long*)take();
+  P.solver_ws = take();
+  P.solver_ws_bytes = solver_ws_bytes(int(C));
+  P.render = (float*)take();
+  P.sc = (SimScalars*)take();
+  s->export_buf = (float*)take();
+  int nn = g.n;
+  cudaMemcpyAsync(P.start + g.nbins, &nn, 4, cudaMemcpyHostToDevice, s->st);
+  // initial scalars
+  SimScalars& hs = s->hs;
+  std::memset(&hs, 0, sizeof hs);
+  hs.motion = cfg->motion;
+  hs.ctl.phase = cfg->motion.kind == PL_MOTION_STILL    ? PL_PHASE_DONE
+                 : cfg->motion.kind == PL_MOTION_MANUAL ? PL_PHASE_MANUAL
+                                                        : PL_PHASE_WAIT;
+  hs.counts[0] = g.n;
+  hs.interior = 1;
+  rc = push_scalars(s);
+  if (!rc) {
+    std::vector<double> zero;
+    rc = upload_parcels(s, init.x.data(), init.y.data(), init.z.data(), nullptr, nullptr, nullptr, nullptr);
+  }
+  if (!rc) rc = build_graph(s);
+  if (rc) {
+    std::string msg = g_err;
+    pl_destroy(s);
+    g_err = msg;
+    return rc;
+  }
+  *out = s;
+  return PL_OK;
+}
+
+void pl_destroy(pl_sim* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->mem) cudaFree(s->mem);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+int pl_get_sizes(const pl_sim* s, pl_sizes* o) {
+  if (!s || !o) return fail(PL_E_ARG, "pl_get_sizes: null argument");
+  std::memset(o, 0, sizeof *o);
+  o->n = s->g.n;
+  o->nx = s->g.nx;
+  o->ny = s->g.ny;
+  o->nz = s->g.nz;
+  o->h = s->g.h;
+  o->parcel_volume = s->g.parcel_volume;
+  o->pivot_world[0] = s->g.pwx;
+  o->pivot_world[1] = s->g.pwy;
+  o->fill_height = s->fill_height;
+  for (int k = 0; k < 3; k++) o->band_counts[k] = s->band_counts[k];
+  return PL_OK;
+}
+
+int pl_stable_dt(pl_sim* s, double* out) {
+  if (!s || !out) return fail(PL_E_ARG, "pl_stable_dt: null argument");
+  *out = host_stable_dt(s);
+  return PL_OK;
+}
+
+int pl_finished(const pl_sim* s) { return s && host_finished(s) ? 1 : 0; }
+
+int pl_step(pl_sim* s, double dt) {
+  if (!s) return fail(PL_E_ARG, "pl_step: null handle");
+  cudaSetDevice(s->device);
+  s->hs.force_step = 1;
+  s->hs.forced_dt = dt > 0 ? dt : 0;
+  int rc = push_scalars(s);
+  if (rc) return rc;
+  CK(cudaGraphLaunch(s->exec, s->st));
+  return pull_scalars(s);
+}
+
+int pl_advance(pl_sim* s, double duration, pl_diagnostics* out) {
+  if (!s) return fail(PL_E_ARG, "pl_advance: null handle");
+  cudaSetDevice(s->device);
+  const double end = s->hs.time + duration;  // solver3d.ts:282
+  s->hs.end_time = end;
+  s->hs.force_step = 0;
+  int rc = push_scalars(s);
+  if (rc) return rc;
+  for (int guard = 0; guard < 1000000; guard++) {
+    if (!(s->hs.time < end - 1e-12 && !host_finished(s))) break;
+    double remaining = std::min(end, s->g.duration) - s->hs.time;
+    double dt = host_stable_dt(s);
+    long k = (long)std::ceil(remaining / dt * 1.05) + 1;
+    k = std::max(1L, std::min(k, 4096L));
+    for (long i = 0; i < k; i++) CK(cudaGraphLaunch(s->exec, s->st));
+    rc = pull_scalars(s);
+    if (rc) return rc;
+  }
+  return out ? pl_get_diagnostics(s, out) : PL_OK;
+}
+
+int pl_sync(pl_sim* s) {
+  if (!s) return fail(PL_E_ARG, "pl_sync: null handle");
+  cudaSetDevice(s->device);
+  return pull_scalars(s);
+}
+
+int pl_set_tilt_target(pl_sim* s, double angle_deg, double time) {  // motion.ts:40-44
+  if (!s) return fail(PL_E_ARG, "pl_set_tilt_target: null handle");
+  (void)time;
+  double a = std::max(0.0, std::min(s->hs.motion.max_angle_deg, angle_deg));
+  s->hs.ctl.target = a * DEG;
+  return push_scalars(s);
+}
+
+int pl_controller(const pl_sim* s, double* angle_deg, int32_t* phase) {
+  if (!s) return fail(PL_E_ARG, "pl_controller: null handle");
+  if (angle_deg) *angle_deg = s->hs.ctl.angle / DEG;
+  if (phase) *phase = s->hs.ctl.phase;
+  return PL_OK;
+}
+
+int pl_get_diagnostics(pl_sim* s, pl_diagnostics* d) {  // solver3d.ts:796-814
+  if (!s || !d) return fail(PL_E_ARG, "pl_get_diagnostics: null argument");
+  const SimScalars& h = s->hs;
+  const double v = s->g.parcel_volume * 2 * 1e6;
+  std::memset(d, 0, sizeof *d);
+  d->time = h.time;
+  d->steps = h.steps;
+  d->angle_deg = h.ctl.angle / DEG;
+  d->phase = h.ctl.phase;
+  d->particles = s->g.n;
+  d->grid[0] = s->g.nx;
+  d->grid[1] = s->g.ny;
+  d->grid[2] = s->g.nz;
+  d->pressure_iterations = h.last_iters;
+  d->pressure_failures = h.failures;
+  d->correction_iterations = h.corr_iters;
+  d->discharged_ml = h.counts[1] * v;
+  d->spilled_ml = h.counts[2] * v;
+  d->lost_ml = h.counts[3] * v;
+  d->in_pot_ml = h.counts[0] * v;
+  double md;
+  std::memcpy(&md, &h.max_div_bits, 8);
+  d->max_divergence = md / s->g.h;
+  d->interior_density = h.interior;
+  return PL_OK;
+}
+
+int pl_discharged_fractions(pl_sim* s, double out[3]) {  // solver3d.ts:817-823
+  if (!s || !out) return fail(PL_E_ARG, "pl_discharged_fractions: null argument");
+  const int* c = s->hs.by_origin;
+  int n = c[0] + c[1] + c[2];
+  if (n == 0) return PL_NONE;
+  for (int k = 0; k < 3; k++) out[k] = double(c[k]) / double(n);
+  return PL_OK;
+}
+
+int pl_read_particles(pl_sim* s, float* pos4, float* vel4, uint32_t* status) {
+  if (!s) return fail(PL_E_ARG, "pl_read_particles: null handle");
+  std::vector<float4> pos, vel;
+  int rc = download_parcels(s, pos, vel);
+  if (rc) return rc;
+  for (int p = 0; p < s->g.n; p++) {
+    if (pos4) {
+      pos4[4 * p] = pos[p].x;
+      pos4[4 * p + 1] = pos[p].y;
+      pos4[4 * p + 2] = pos[p].z;
+      pos4[4 * p + 3] = 0.f;
+    }
+    if (vel4) {
+      vel4[4 * p] = vel[p].x;
+      vel4[4 * p + 1] = vel[p].y;
+      vel4[4 * p + 2] = vel[p].z;
+      vel4[4 * p + 3] = 0.f;
+    }
+    if (status) {
+      int meta;
+      std::memcpy(&meta, &vel[p].w, 4);
+      status[p] = uint32_t(meta & 0xff);
+    }
+  }
+  return PL_OK;
+}
+
+int pl_read_particles_f64(pl_sim* s, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                          uint8_t* status) {
+  if (!s) return fail(PL_E_ARG, "pl_read_particles_f64: null handle");
+  std::vector<float4> pos, vel;
+  int rc = download_parcels(s, pos, vel);
+  if (rc) return rc;
+  for (int p = 0; p < s->g.n; p++) {
+    if (x) x[p] = pos[p].x;
+    if (y) y[p] = pos[p].y;
+    if (z) z[p] = pos[p].z;
+    if (vx) vx[p] = vel[p].x;
+    if (vy) vy[p] = vel[p].y;
+    if (vz) vz[p] = vel[p].z;
+    if (status) {
+      int meta;
+      std::memcpy(&meta, &vel[p].w, 4);
+      status[p] = uint8_t(meta & 0xff);
+    }
+  }
+  return PL_OK;
+}
+
+int pl_read_origin(const pl_sim* s, uint8_t* origin) {
+  if (!s || !origin) return fail(PL_E_ARG, "pl_read_origin: null argument");
+  std::memcpy(origin, s->origin.data(), s->origin.size());
+  return PL_OK;
+}
+
+int pl_read_render_positions(pl_sim* s, float* xyz6n) {
+  if (!s || !xyz6n) return fail(PL_E_ARG, "pl_read_render_positions: null argument");
+  cudaSetDevice(s->device);
+  launch_render(s->g, s->P, s->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(xyz6n, s->P.render, size_t(s->g.n) * 6 * 4, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return PL_OK;
+}
+
+int pl_get_state(pl_sim* s, pl_sim_state* st) {
+  if (!s || !st) return fail(PL_E_ARG, "pl_get_state: null argument");
+  const SimScalars& h = s->hs;
+  std::memset(st, 0, sizeof *st);
+  st->time = h.time;
+  st->steps = h.steps;
+  st->phi = h.phi;
+  st->omega = h.omega;
+  for (int k = 0; k < 4; k++) st->counts[k] = h.counts[k];
+  for (int k = 0; k < 3; k++) st->discharged_by_origin[k] = h.by_origin[k];
+  st->last_iterations = h.last_iters;
+  st->failures = h.failures;
+  double md;
+  std::memcpy(&md, &h.max_div_bits, 8);
+  st->max_div = md / s->g.h;
+  st->interior = h.interior;
+  const DevController& c = h.ctl;
+  st->controller = pl_controller_state{c.phase,     c.pour,      c.angle,     c.phase_start,     c.start_angle, c.start_rate,
+                                       c.last_rate, c.flow_rate, c.last_discharged, c.target, c.manual_rate};
+  return PL_OK;
+}
+
+int pl_set_state(pl_sim* s, const pl_sim_state* st, const double* x, const double* y, const double* z,
+                 const double* vx, const double* vy, const double* vz, const uint8_t* status) {
+  if (!s) return fail(PL_E_ARG, "pl_set_state: null handle");
+  cudaSetDevice(s->device);
+  SimScalars& h = s->hs;
+  const int n = s->g.n;
+  if (x && y && z && status) {
+    int rc = upload_parcels(s, x, y, z, vx, vy, vz, status);
+    if (rc) return rc;
+    for (int k = 0; k < 4; k++) h.counts[k] = 0;
+    for (int k = 0; k < 3; k++) h.by_origin[k] = 0;
+    double m = 0;
+    for (int p = 0; p < n; p++) {
+      if (status[p] > 3) return fail(PL_E_ARG, "pl_set_state: status %d of parcel %d", status[p], p);
+      h.counts[status[p]]++;
+      if (status[p] == PL_DISCHARGED) h.by_origin[s->origin[p]]++;
+      if (status[p] == PL_IN_POT && vx && vy && vz) {
+        double a = (float)vx[p], b = (float)vy[p], c = (float)vz[p];
+        double sp = a * a + b * b + c * c;
+        if (sp > m) m = sp;
+      }
+    }
+    std::memcpy(&h.max_speed_bits, &m, 8);
+  } else if (x || y || z || status) {
+    return fail(PL_E_ARG, "pl_set_state: x, y, z and status go together");
+  }
+  if (st) {
+    h.time = st->time;
+    h.steps = st->steps;
+    h.phi = st->phi;
+    h.omega = st->omega;
+    h.last_iters = st->last_iterations;
+    h.failures = st->failures;
+    h.interior = st->interior;
+    double md = st->max_div * s->g.h;
+    std::memcpy(&h.max_div_bits, &md, 8);
+    const pl_controller_state& c = st->controller;
+    h.ctl = DevController{c.phase,     c.pour,      c.angle,           c.phase_start, c.start_angle, c.start_rate,
+                          c.last_rate, c.flow_rate, c.last_discharged, c.target,      c.manual_rate};
+  }
+  return push_scalars(s);
+}
+
+int pl_get_field(pl_sim* s, int32_t field, void* out, size_t count) {
+  if (!s || !out) return fail(PL_E_ARG, "pl_get_field: null argument");
+  cudaSetDevice(s->device);
+  const Geo& g = s->g;
+  const size_t C = g.nc, F = g.nf;
+  auto faces = [&](const float* src) -> int {
+    if (count < F) return fail(PL_E_ARG, "pl_get_field: buffer holds %zu of %zu", count, F);
+    std::vector<float> tmp(F);
+    CK(cudaMemcpyAsync(tmp.data(), src, F * 4, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    double* o = static_cast<double*>(out);
+    for (size_t i = 0; i < F; i++) o[i] = tmp[i];
+    return PL_OK;
+  };
+  auto listed = [&](const double* src) -> int {  // list-indexed -> grid, zero off the list
+    if (count < C) return fail(PL_E_ARG, "pl_get_field: buffer holds %zu of %zu", count, C);
+    int m = s->hs.m;
+    std::vector<int> list(std::max(m, 1));
+    std::vector<double> v(std::max(m, 1));
+    if (m > 0) {
+      CK(cudaMemcpyAsync(list.data(), s->P.list, size_t(m) * 4, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaMemcpyAsync(v.data(), src, size_t(m) * 8, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+    }
+    double* o = static_cast<double*>(out);
+    std::fill(o, o + C, 0.0);
+    for (int t = 0; t < m; t++) o[list[t]] = v[t];
+    return PL_OK;
+  };
+  switch (field) {
+    case PL_FIELD_CELL:
+      if (count < C) return fail(PL_E_ARG, "pl_get_field: buffer holds %zu of %zu", count, C);
+      CK(cudaMemcpyAsync(out, s->P.cell, C, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      return PL_OK;
+    case PL_FIELD_VELOCITY:
+      return faces(s->P.u);
+    case PL_FIELD_VELOCITY_PREV:
+      return faces(s->P.uprev);
+    case PL_FIELD_PRESSURE:
+      return listed(s->P.q);
+    case PL_FIELD_CORRECTION:
+      launch_export_correction(g, s->P, s->export_buf, s->st);
+      CK(cudaGetLastError());
+      return faces(s->export_buf);
+    case PL_FIELD_VALID:
+      if (count < F) return fail(PL_E_ARG, "pl_get_field: buffer holds %zu of %zu", count, F);
+      CK(cudaMemcpyAsync(out, s->P.valid, F, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      return PL_OK;
+    case PL_FIELD_DENSITY:
+      return listed(s->P.density);
+    case PL_FIELD_RHS:
+      return listed(s->P.rhs);
+    default:
+      return fail(PL_E_ARG, "pl_get_field: unknown field %d", field);
+  }
+}
+
+int pl_pcg_solve_device(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny, int32_t nz,
+                        double tol, int32_t max_iter, int32_t preconditioner, int32_t precision, void* stream,
+                        int32_t* iterations, int32_t* converged, double* residual) {
+  if (!cell || !b || !q) return fail(PL_E_ARG, "pl_pcg_solve_device: null buffer");
+  char err[256] = "";
+  int rc = standalone_pcg(cell, b, q, nx, ny, nz, tol, max_iter, preconditioner, precision, (cudaStream_t)stream,
+                          iterations, converged, residual, err, sizeof err);
+  if (rc) return fail(rc, "%s", err);
+  return PL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,55 @@
+// Launch helpers and sizes shared by kernels.cu, solver.cu and engine.cu.
+#pragma once
+
+#include "common.cuh"
+
+namespace pl {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr int SCAN_MAX_TILES = 4096;  // bins <= 8M
+constexpr int DENSITY_BLOCKS = 148;
+constexpr int SOLVER_THREADS = 1024;
+constexpr int MAX_LEVELS = 2048;  // wavefronts i+j+k of the MIC(0) sweeps
+
+// List-indexed scratch of the pressure solves (capacity = interior cells).
+struct SolverWs {
+  int cap;
+  int* nb;        // 6 * cap: list index of the -x,+x,-y,+y,-z,+z neighbour or -1
+  double* adiag;  // non-solid neighbour count
+  int* wave;      // i + j + k
+  int* order;     // list entries by wavefront
+  int* lstart;    // MAX_LEVELS + 1 wavefront starts
+  int* nlev;      // [0] wavefront count, [1] lowest wavefront
+  double* pc;     // MIC(0) inverse-sqrt diagonal
+  double* bp;     // pressure rhs (negative divergence)
+  double *r, *z, *s, *as, *qv;
+};
+
+struct SolveArgs {
+  const double* b;
+  double* q;
+  double tol;
+  int max_iter;
+  int is_correction;  // density solve: gated by corr_any, records corr_iters and the interior mean
+  int factor;         // build the wavefront order and the MIC(0) factor first
+};
+
+SolverWs solver_ws_carve(void* base, int cap);
+size_t solver_ws_bytes(int cap);
+
+void launch_substep_front(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_substep_middle(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_substep_back(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_render(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_export_correction(const Geo& g, const DevPtrs& P, float* out, cudaStream_t st);
+
+// Standalone Pcg3D.solve on a caller's grid (pl_pcg_solve_device).
+int standalone_pcg(const uint8_t* cell, const double* b, double* q, int nx, int ny, int nz, double tol,
+                   int max_iter, int precond, int precision, cudaStream_t st, int* iterations, int* converged,
+                   double* residual, char* err, size_t errlen);
+
+}  // namespace pl

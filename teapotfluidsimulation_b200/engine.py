@@ -1,0 +1,266 @@
+"""Python host side of the B200 pour engine, mirroring the reference's solver surface.
+
+`Simulation3D` here has the members of PourLab's `Simulation3D` (src/sim3d/solver3d.ts:62-824) and
+`GpuSimulation3D` (src/gpu3d/solver.ts:89-490) that callers use: construct from a config, `step`,
+`advance`, `stable_dt`, `finished`, `diagnostics`, `discharged_fractions`, `read_particles`,
+`read_render_positions`, the controller's `set_target` (setTilt) and the state accessors the
+verification harness needs. Every call goes through the C ABI of libpourlab_cuda.so
+(include/pourlab.h); there is no CPU fallback, and a missing library is an ImportError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpourlab_cuda.so")
+
+_lib = None
+
+EXPORTED = [
+    "pl_default_teapot", "pl_default_motion", "pl_gentle_pour", "pl_create", "pl_destroy", "pl_last_error",
+    "pl_get_sizes", "pl_stable_dt", "pl_finished", "pl_step", "pl_advance", "pl_sync", "pl_set_tilt_target",
+    "pl_controller", "pl_get_diagnostics", "pl_discharged_fractions", "pl_read_particles",
+    "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
+    "pl_get_field", "pl_pcg_solve_device",
+]
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pourlab error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Load libpourlab_cuda.so (built by __graft_entry__.build()); raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build the CUDA engine first (python -c "
+                          f"'import __graft_entry__ as g; g.build()')")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
+    u8p = C.POINTER(C.c_uint8)
+    L.pl_default_teapot.argtypes = [C.POINTER(abi.Teapot)]
+    L.pl_default_teapot.restype = None
+    L.pl_default_motion.argtypes = [C.POINTER(abi.Motion)]
+    L.pl_default_motion.restype = None
+    L.pl_gentle_pour.argtypes = [C.c_double, C.c_double, C.POINTER(abi.Config)]
+    L.pl_gentle_pour.restype = None
+    L.pl_create.argtypes = [C.POINTER(abi.Config), C.POINTER(P)]
+    L.pl_destroy.argtypes = [P]
+    L.pl_destroy.restype = None
+    L.pl_last_error.argtypes = []
+    L.pl_last_error.restype = C.c_char_p
+    L.pl_get_sizes.argtypes = [P, C.POINTER(abi.Sizes)]
+    L.pl_stable_dt.argtypes = [P, dp]
+    L.pl_finished.argtypes = [P]
+    L.pl_step.argtypes = [P, C.c_double]
+    L.pl_advance.argtypes = [P, C.c_double, C.POINTER(abi.Diagnostics)]
+    L.pl_sync.argtypes = [P]
+    L.pl_set_tilt_target.argtypes = [P, C.c_double, C.c_double]
+    L.pl_controller.argtypes = [P, dp, C.POINTER(C.c_int32)]
+    L.pl_get_diagnostics.argtypes = [P, C.POINTER(abi.Diagnostics)]
+    L.pl_discharged_fractions.argtypes = [P, dp]
+    L.pl_read_particles.argtypes = [P, fp, fp, C.POINTER(C.c_uint32)]
+    L.pl_read_particles_f64.argtypes = [P, dp, dp, dp, dp, dp, dp, u8p]
+    L.pl_read_origin.argtypes = [P, u8p]
+    L.pl_read_render_positions.argtypes = [P, fp]
+    L.pl_get_state.argtypes = [P, C.POINTER(abi.SimState)]
+    L.pl_set_state.argtypes = [P, C.POINTER(abi.SimState), dp, dp, dp, dp, dp, dp, u8p]
+    L.pl_get_field.argtypes = [P, C.c_int32, P, C.c_size_t]
+    L.pl_pcg_solve_device.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                                      C.c_int32, P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp]
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> int:
+    if rc < 0:
+        raise EngineError(rc, lib().pl_last_error().decode())
+    return rc
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def gentle_pour(cell_mm: float, seconds: float, **over) -> abi.Config:
+    """gentlePour3D(cellMm, seconds) (src/sim3d/presets3d.ts:9-26) with keyword overrides."""
+    return abi.gentle_pour(cell_mm, seconds, **over)
+
+
+class Simulation3D:
+    """The pour simulation on one B200 (the reference's Simulation3D / GpuSimulation3D surface)."""
+
+    def __init__(self, cfg: abi.Config):
+        L = lib()
+        self._h = C.c_void_p()
+        _check(L.pl_create(C.byref(cfg), C.byref(self._h)))
+        self.cfg = cfg
+        s = abi.Sizes()
+        _check(L.pl_get_sizes(self._h, C.byref(s)))
+        self.sizes = s
+        self.n, self.nx, self.ny, self.nz = s.n, s.nx, s.ny, s.nz
+        self.h = s.h
+        self.parcel_volume = s.parcel_volume
+        self.pivot_world = (s.pivot_world[0], s.pivot_world[1])
+        self.fill_height = s.fill_height
+        self.band_counts = [s.band_counts[0], s.band_counts[1], s.band_counts[2]]
+
+    # ------------------------------------------------------------ lifetime
+    def destroy(self):
+        """GpuSimulation3D.destroy() (src/gpu3d/solver.ts:486-489)."""
+        if self._h:
+            lib().pl_destroy(self._h)
+            self._h = C.c_void_p()
+
+    close = destroy
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # ------------------------------------------------------------ sizes
+    @property
+    def nc(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def nfaces(self) -> int:
+        nx, ny, nz = self.nx, self.ny, self.nz
+        return (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+
+    # ------------------------------------------------------------ stepping
+    def stable_dt(self) -> float:
+        """stableDt() (solver3d.ts:268-278)."""
+        out = C.c_double()
+        _check(lib().pl_stable_dt(self._h, C.byref(out)))
+        return out.value
+
+    @property
+    def finished(self) -> bool:
+        return bool(lib().pl_finished(self._h))
+
+    def step(self, dt: float = -1.0):
+        """step(dt) (solver3d.ts:288-309); dt <= 0 uses min(stableDt(), duration - time)."""
+        _check(lib().pl_step(self._h, dt))
+
+    def advance(self, duration: float) -> dict:
+        """advance(duration) (solver3d.ts:281-286): whole stable substeps; returns diagnostics()."""
+        d = abi.Diagnostics()
+        _check(lib().pl_advance(self._h, duration, C.byref(d)))
+        return d.as_dict()
+
+    def sync(self):
+        _check(lib().pl_sync(self._h))
+
+    # ------------------------------------------------------------ controller
+    def set_target(self, angle_deg: float, time: float | None = None):
+        """controller.setTarget(angleDeg, time) (src/sim/motion.ts:40-44): the setTilt of a manual pour."""
+        t = self.diagnostics()["time"] if time is None else time
+        _check(lib().pl_set_tilt_target(self._h, angle_deg, t))
+
+    set_tilt = set_target
+
+    def controller(self) -> tuple[float, str]:
+        a = C.c_double()
+        ph = C.c_int32()
+        _check(lib().pl_controller(self._h, C.byref(a), C.byref(ph)))
+        return a.value, abi.PHASES[ph.value]
+
+    # ------------------------------------------------------------ results
+    def diagnostics(self) -> dict:
+        """diagnostics() (solver3d.ts:796-814)."""
+        d = abi.Diagnostics()
+        _check(lib().pl_get_diagnostics(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def discharged_fractions(self):
+        """dischargedFractions() (solver3d.ts:817-823): None before anything poured."""
+        out = np.zeros(3)
+        rc = _check(lib().pl_discharged_fractions(self._h, _ptr(out, C.c_double)))
+        return None if rc == abi.PL_NONE else out
+
+    def read_particles(self) -> dict:
+        """readParticles() (src/gpu3d/solver.ts:409-428): pos/vel as float4 rows, status u32."""
+        n = self.n
+        pos = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        st = np.zeros(n, np.uint32)
+        _check(lib().pl_read_particles(self._h, _ptr(pos, C.c_float), _ptr(vel, C.c_float), _ptr(st, C.c_uint32)))
+        return {"pos": pos, "vel": vel, "status": st}
+
+    def particles(self) -> dict:
+        """Parcel state as FP64 SoA in id order (the arrays Simulation3D exposes)."""
+        n = self.n
+        a = {k: np.zeros(n) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        st = np.zeros(n, np.uint8)
+        _check(lib().pl_read_particles_f64(self._h, *[_ptr(a[k], C.c_double) for k in ("x", "y", "z", "vx", "vy", "vz")],
+                                           _ptr(st, C.c_uint8)))
+        a["status"] = st
+        return a
+
+    def origin(self) -> np.ndarray:
+        o = np.zeros(self.n, np.uint8)
+        _check(lib().pl_read_origin(self._h, _ptr(o, C.c_uint8)))
+        return o
+
+    def read_render_positions(self) -> np.ndarray:
+        """readRenderPositions() (src/gpu3d/solver.ts:443-475): xyz of the half, then the mirror."""
+        out = np.zeros(6 * self.n, np.float32)
+        _check(lib().pl_read_render_positions(self._h, _ptr(out, C.c_float)))
+        return out
+
+    # ------------------------------------------------------------ state (parity harness)
+    def get_state(self) -> abi.SimState:
+        st = abi.SimState()
+        _check(lib().pl_get_state(self._h, C.byref(st)))
+        return st
+
+    def set_state(self, st: abi.SimState | None, parts: dict | None):
+        ptrs = [None] * 7
+        if parts is not None:
+            keep = [np.ascontiguousarray(parts[k], dtype=np.float64) for k in ("x", "y", "z", "vx", "vy", "vz")]
+            stat = np.ascontiguousarray(parts["status"], dtype=np.uint8)
+            ptrs = [_ptr(k, C.c_double) for k in keep] + [_ptr(stat, C.c_uint8)]
+        _check(lib().pl_set_state(self._h, C.byref(st) if st is not None else None, *ptrs))
+
+    def field(self, which: int) -> np.ndarray:
+        n = self.nfaces if which in abi.FACE_FIELDS else self.nc
+        dtype = np.uint8 if which in abi.U8_FIELDS else np.float64
+        out = np.zeros(n, dtype)
+        _check(lib().pl_get_field(self._h, which, out.ctypes.data_as(C.c_void_p), n))
+        return out
+
+
+def pcg_solve_device(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny: int, nz: int, tol: float, max_iter: int,
+                     preconditioner: int = abi.PRECOND_MIC0, precision: int = abi.SOLVE_F64, stream: int = 0):
+    """Pcg3D.solve on device buffers (pl_pcg_solve_device): returns (iterations, converged, residual)."""
+    it = C.c_int32()
+    conv = C.c_int32()
+    res = C.c_double()
+    _check(lib().pl_pcg_solve_device(C.c_void_p(cell_ptr), C.c_void_p(b_ptr), C.c_void_p(q_ptr), nx, ny, nz, tol,
+                                     max_iter, preconditioner, precision, C.c_void_p(stream), C.byref(it),
+                                     C.byref(conv), C.byref(res)))
+    return it.value, bool(conv.value), res.value
