@@ -1,0 +1,366 @@
+"""Benchmark of the B200 pour engine: simulated seconds per wall second of the 4 mm gentle pour.
+
+One step is one substep of the pour (binning, particle-to-grid, pressure solve, extrapolation,
+density correction, advection). The timed region runs K substeps after W warm-up substeps, each
+substep timed on the engine's stream with CUDA events (the graph's first and last stage events),
+with a 256 MiB buffer written between substeps so every substep starts with a cold L2. The
+reported value is the simulated time those K substeps covered divided by their summed device time.
+
+`e2e` repeats the measurement through the public C ABI call a host program makes per substep
+(pl_step: host->device control block, the substep, device->host stats block), timed by the host
+clock around each call. The reference arm (--impl reference) times the CPU FP64 restatement of the
+reference solver on the same workload (the reference itself is TypeScript and no JavaScript
+runtime exists on the box).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: torchrun --nproc-per-node N bench.py --gpus N: every rank runs its own replica of the
+pour (the single pour does not shard); value is the sum over ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "gentle 400 mL pour, 4 mm cells, half pot (81x81x22 grid, 88,856 parcels), seed 1"
+KERNELS_PER_SUBSTEP = 13  # controller, bin count/scan/place/permute, p2g, solve setup, pcg, 2x extrapolation,
+#                           density, correction pcg, advect
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cell-mm", type=float, default=4.0)
+    ap.add_argument("--precond", default="mic0", choices=["mic0", "mg"])
+    ap.add_argument("--start", type=float, default=0.0, help="simulated seconds to advance before warm-up")
+    ap.add_argument("--cpu-sample", type=int, default=60, help="substeps of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def make_cfg(args):
+    from teapotfluidsimulation_b200 import abi
+
+    cfg = abi.gentle_pour(args.cell_mm, 20.0)
+    cfg.preconditioner = abi.PRECOND_MG if args.precond == "mg" else abi.PRECOND_MIC0
+    return cfg
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allmax(x: float, world: int, device: str = "cuda") -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(x: float, world: int, device: str = "cuda") -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = float(p[2])
+                except ValueError:
+                    continue
+                for name, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the pressure PCG kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "pcg_pressure_ncu.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch:\s*([0-9.eE+]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+def pcg_bytes_per_iteration(m: int) -> float:
+    """Algorithmic bytes of one FP64 MIC(0)-PCG iteration over m liquid cells.
+
+    Each array counted once per logical pass: apply A (s, 6 neighbour indices, diagonal, write As:
+    8+24+8+8), s.As (16), q/r update (read q, s, r, As, write q, r: 48), the two MIC(0) sweeps
+    (r or qv, pc, 3 neighbour indices, 3 neighbour values, write: 2 x 48), z.r (16), direction
+    update (read z, s, write s: 24). Total 248 bytes per liquid cell.
+    """
+    return 248.0 * m
+
+
+def run_cpu_baseline(args, substeps: int) -> dict:
+    """The CPU FP64 restatement of the reference solver on a bounded sample of the same workload."""
+    from oracle import oracle as O
+
+    sim = O.OracleSim(make_cfg(args))
+    if args.start > 0:
+        sim.advance(args.start)
+    t_sim0 = sim.diagnostics()["time"]
+    t0 = time.perf_counter()
+    for _ in range(substeps):
+        sim.step(-1.0)
+    wall = time.perf_counter() - t0
+    t_sim = sim.diagnostics()["time"] - t_sim0
+    sim.close()
+    return {"value": t_sim / wall, "unit": "sim-s/wall-s", "cores": 1, "kind": "port",
+            "sample": f"{substeps} substeps of the same pour from t={args.start:g} s, C++ FP64 restatement "
+                      f"of src/sim3d (one thread; the reference is single-threaded TypeScript)",
+            "wall_s": wall, "sim_s": t_sim, "ms_per_substep": 1000 * wall / substeps}
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    sim = O.OracleSim(make_cfg(args))
+    if args.start > 0:
+        sim.advance(args.start)
+    for _ in range(args.warmup):
+        sim.step(-1.0)
+    t_sim0 = sim.diagnostics()["time"]
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(-1.0)
+    wall = time.perf_counter() - t0
+    t_sim = sim.diagnostics()["time"] - t_sim0
+    value = t_sim / wall
+    line = {
+        "impl": "reference", "metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "substeps_timed": args.steps,
+                   "note": "C++ FP64 restatement of the reference CPU solver (TypeScript reference not runnable: "
+                           "no JavaScript runtime)"},
+        "cpu_baseline": {"value": value, "unit": "sim-s/wall-s", "cores": 1, "kind": "port",
+                         "sample": f"{args.steps} substeps after {args.warmup} warm-up substeps"},
+        "e2e": {"value": value, "unit": "sim-s/wall-s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import ctypes
+
+    import torch
+
+    world, rank, local = dist_init()
+    import teapotfluidsimulation_b200 as pkg
+    from teapotfluidsimulation_b200 import abi
+
+    torch.cuda.set_device(local)
+    cfg = make_cfg(args)
+    cfg.device = local
+    sim = pkg.Simulation3D(cfg)
+    if args.start > 0:
+        sim.advance(args.start)
+    sim.enable_stage_timing(True)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+
+    def substep(stage_acc):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        sim.enqueue(1)
+        sim.sync()
+        st = sim.stage_times()
+        if stage_acc is not None:
+            for k, v in st.items():
+                stage_acc[k] = stage_acc.get(k, 0.0) + v
+        return sum(st.values())
+
+    for _ in range(args.warmup):
+        substep(None)
+    d0 = sim.diagnostics()
+    stage_acc: dict = {}
+    pcg_work = 0.0
+    iters = []
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_ms = 0.0
+    steps_done = 0
+    for _ in range(args.steps):
+        if sim.finished:
+            break
+        dev_ms += substep(stage_acc)
+        steps_done += 1
+        d = sim.diagnostics()
+        iters.append(d["pressureIterations"])
+        pcg_work += pcg_bytes_per_iteration(d["liquidCells"]) * d["pressureIterations"]
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    d1 = sim.diagnostics()
+    sim_s = d1["time"] - d0["time"]
+    max_ms = allmax(dev_ms, world)
+    total_sim = allsum(sim_s, world)
+    value = total_sim / (max_ms / 1000.0)
+
+    # end to end through the C ABI: pl_step per substep on a second replica from the same start
+    e2e_sim = pkg.Simulation3D(make_cfg(args) if world == 1 else cfg)
+    if args.start > 0:
+        e2e_sim.advance(args.start)
+    for _ in range(args.warmup):
+        e2e_sim.step(-1.0)
+    e0 = e2e_sim.diagnostics()["time"]
+    wall = 0.0
+    for _ in range(steps_done):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_sim.step(-1.0)
+        wall += time.perf_counter() - t0
+    e2e_s = e2e_sim.diagnostics()["time"] - e0
+    e2e_value = allsum(e2e_s, world) / allmax(wall, world)
+    scalars = 400  # bytes of the device scalar block (SimScalars) copied each way per pl_step
+
+    peaks, peak_kind = measured_peaks()
+    pres_ms = stage_acc.get("pressure", 0.0) / max(steps_done, 1)
+    achieved = (pcg_work / max(steps_done, 1)) / (pres_ms / 1000.0) / 1e9 if pres_ms > 0 else 0.0
+    traffic = profile_traffic()
+    line = {
+        "metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s", "n_gpus": world, "steps": steps_done,
+        "warmup": args.warmup, "ms_per_step": max_ms / max(steps_done, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve / f32 parcels and faces", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "preconditioner": args.precond,
+                   "start_s": args.start, "simulated_s": sim_s, "l2": "256 MiB buffer written between substeps",
+                   "parallelism": f"replicas x{world}"},
+        "pressure_ms_per_substep": pres_ms,
+        "pressure_iterations_mean": (sum(iters) / len(iters)) if iters else 0,
+        "stages_ms_per_substep": {k: v / max(steps_done, 1) for k, v in stage_acc.items()},
+        "gpu_launches": KERNELS_PER_SUBSTEP * steps_done,
+        "e2e": {"value": e2e_value, "unit": "sim-s/wall-s", "h2d_bytes_per_step": scalars,
+                "d2h_bytes_per_step": scalars},
+        "roofline": {"kernel": "k_pcg (pressure solve, with its setup)", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": achieved / peaks.get("hbm_gbs", 1.0), "peak_kind": peak_kind,
+                     "traffic": traffic},
+    }
+    if clk:
+        line["clocks"] = clk
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = run_cpu_baseline(args, args.cpu_sample)
+    if rank == 0:
+        print(json.dumps(line))
+    e2e_sim.destroy()
+    sim.destroy()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

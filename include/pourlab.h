@@ -112,7 +112,8 @@ typedef struct pl_config {
   /* engine settings (no counterpart in Config3D) */
   int32_t preconditioner;  /* enum pl_preconditioner */
   int32_t solve_precision; /* enum pl_solve_precision */
-  int32_t reserved[6];
+  int32_t device;          /* CUDA device ordinal; -1 = the calling thread's current device */
+  int32_t reserved[5];
 } pl_config;
 
 /* Diagnostics3D (src/sim3d/solver3d.ts:45-60). */
@@ -132,6 +133,8 @@ typedef struct pl_diagnostics {
   double in_pot_ml;
   double max_divergence; /* 1/s, after projection */
   double interior_density;
+  int32_t liquid_cells; /* unknowns of the last pressure solve (engine extension) */
+  int32_t reserved;
 } pl_diagnostics;
 
 /* Constructor-derived sizes (solver3d.ts:62-84, 116-228). */
@@ -206,6 +209,10 @@ typedef struct pl_sim pl_sim;
  * (src/sim3d/solver3d.ts:116-228, src/gpu3d/solver.ts:108-124). Seeding, banding and grid sizing
  * run on the host in FP64 exactly as the reference constructor; the state then moves to the GPU. */
 int pl_create(const pl_config* cfg, pl_sim** out);
+/* The host part of that constructor alone, without a device: grid sizes, pivot, parcel volume and
+ * band counts, and, where the pointers are not NULL, the seeded parcel positions (FP64, id order)
+ * and origin layers (solver3d.ts:116-228). Call with NULL arrays first to learn n. */
+int pl_plan(const pl_config* cfg, pl_sizes* out, double* x, double* y, double* z, uint8_t* origin);
 /* GpuSimulation3D.destroy() (src/gpu3d/solver.ts:486-489). Accepts NULL. */
 void pl_destroy(pl_sim* sim);
 /* Message of the last failing call on this thread ("" if none). */
@@ -233,6 +240,31 @@ int pl_step(pl_sim* sim, double dt);
 int pl_advance(pl_sim* sim, double duration, pl_diagnostics* out);
 /* Wait for queued device work (GpuSimulation3D.sync, src/gpu3d/solver.ts:289-294). */
 int pl_sync(pl_sim* sim);
+/* Queue `count` stable substeps without waiting (the pipelined GpuSimulation3D.step,
+ * src/gpu3d/solver.ts:296-370, with the controller on the device instead of one substep behind).
+ * Substeps past the end of the run do nothing. pl_sync makes the host-side state current. */
+int pl_enqueue_substeps(pl_sim* sim, int32_t count);
+/* The CUDA stream (cudaStream_t) the handle runs on, for callers that order their own work
+ * (timing events, buffer fills) with the engine's. */
+void* pl_stream(const pl_sim* sim);
+
+/* ------------------------------------------------------------------ stage timing */
+
+/* Stages of one substep, in order. */
+enum pl_stage {
+  PL_STAGE_BIN = 0,      /* controller, binning, classification, liquid list */
+  PL_STAGE_P2G = 1,      /* particle-to-grid, gravity, wall faces */
+  PL_STAGE_PRESSURE = 2, /* pressure solve (setup + PCG) */
+  PL_STAGE_EXTRAP = 3,   /* gradient update and two extrapolation layers */
+  PL_STAGE_DENSITY = 4,  /* density, correction rhs, divergence check */
+  PL_STAGE_CORRECTION = 5, /* density-correction solve */
+  PL_STAGE_ADVECT = 6,   /* grid-to-particle, advection, collisions, accounting */
+  PL_STAGES = 7
+};
+/* Record CUDA events between the stages of every substep (rebuilds the substep graph). */
+int pl_enable_stage_timing(pl_sim* sim, int32_t on);
+/* Device milliseconds per stage of the last completed substep (needs stage timing on). */
+int pl_stage_times(pl_sim* sim, float ms[PL_STAGES]);
 
 /* ------------------------------------------------------------------ controller */
 

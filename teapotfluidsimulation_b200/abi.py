@@ -86,7 +86,8 @@ class Config(C.Structure):
         ("duration", C.c_double),
         ("preconditioner", C.c_int32),
         ("solve_precision", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("device", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -107,6 +108,8 @@ class Diagnostics(C.Structure):
         ("in_pot_ml", C.c_double),
         ("max_divergence", C.c_double),
         ("interior_density", C.c_double),
+        ("liquid_cells", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -127,6 +130,7 @@ class Diagnostics(C.Structure):
             "correctionIterations": self.correction_iterations,
             "maxDivergence": self.max_divergence,
             "interiorDensity": self.interior_density,
+            "liquidCells": self.liquid_cells,
         }
 
 
@@ -228,6 +232,7 @@ def gentle_pour(cell_mm: float, seconds: float, **over) -> Config:
     c.duration = seconds
     c.preconditioner = PRECOND_MIC0
     c.solve_precision = SOLVE_F64
+    c.device = -1
     for k, v in over.items():
         if k == "motion":
             for mk, mv in v.items():

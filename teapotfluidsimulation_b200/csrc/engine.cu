@@ -7,6 +7,7 @@
 // the requested duration has elapsed; substeps launched past the end return immediately.
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -57,13 +58,23 @@ struct pl_sim {
   std::vector<uint8_t> origin;
   pl_config cfg{};
   float* export_buf = nullptr;  // F floats for exported face fields
+  SimScalars* pinned = nullptr; // page-locked staging of the scalar block
+  int timing = 0;
+  int pending = 0;  // substeps queued by pl_enqueue_substeps since the last pull
+  cudaEvent_t ev[PL_STAGES + 1] = {};
 };
 
 namespace {
+int pull_scalars(pl_sim* s);
+
+// Bring the host mirror up to date before a call reads it or writes it back to the device.
+int settle(pl_sim* s) { return s->pending ? pull_scalars(s) : PL_OK; }
 
 int pull_scalars(pl_sim* s) {
-  CK(cudaMemcpyAsync(&s->hs, s->P.sc, sizeof(SimScalars), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaMemcpyAsync(s->pinned, s->P.sc, sizeof(SimScalars), cudaMemcpyDeviceToHost, s->st));
   CK(cudaStreamSynchronize(s->st));
+  std::memcpy(&s->hs, s->pinned, sizeof(SimScalars));
+  s->pending = 0;
   if (s->hs.errors) {
     int e = s->hs.errors;
     return fail(PL_E_TIMEOUT, "device error flags 0x%x (%s%s)", e, (e & ERR_SCAN_TIMEOUT) ? "bin scan wait gave up " : "",
@@ -73,20 +84,43 @@ int pull_scalars(pl_sim* s) {
 }
 
 int push_scalars(pl_sim* s) {
-  CK(cudaMemcpyAsync(s->P.sc, &s->hs, sizeof(SimScalars), cudaMemcpyHostToDevice, s->st));
+  std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
+  CK(cudaMemcpyAsync(s->P.sc, s->pinned, sizeof(SimScalars), cudaMemcpyHostToDevice, s->st));
   CK(cudaStreamSynchronize(s->st));
   return PL_OK;
 }
 
+// One substep, stage by stage; with timing on, an event is recorded at every stage boundary (event
+// record nodes inside the graph).
 void record_substep(pl_sim* s) {
-  launch_substep_front(s->g, s->P, s->st);
-  launch_pressure_solve(s->g, s->P, s->st);
-  launch_substep_middle(s->g, s->P, s->st);
-  launch_correction_solve(s->g, s->P, s->st);
-  launch_substep_back(s->g, s->P, s->st);
+  const Geo& g = s->g;
+  const DevPtrs& P = s->P;
+  cudaStream_t st = s->st;
+  auto mark = [&](int i) {  // external: becomes an event-record node of the captured graph
+    if (s->timing) cudaEventRecordWithFlags(s->ev[i], st, cudaEventRecordExternal);
+  };
+  mark(0);
+  launch_stage_bin(g, P, st);
+  mark(1);
+  launch_stage_p2g(g, P, st);
+  mark(2);
+  launch_pressure_solve(g, P, st);
+  mark(3);
+  launch_stage_extrap(g, P, st);
+  mark(4);
+  launch_stage_density(g, P, st);
+  mark(5);
+  launch_correction_solve(g, P, st);
+  mark(6);
+  launch_stage_advect(g, P, st);
+  mark(7);
 }
 
 int build_graph(pl_sim* s) {
+  if (s->exec) {
+    cudaGraphExecDestroy(s->exec);
+    s->exec = nullptr;
+  }
   cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
   record_substep(s);
@@ -166,7 +200,7 @@ void pl_default_motion(pl_motion* m) {
   m->return_duration = 1.2;
   m->max_hold = 20;  // gentlePour3D overrides the default 12 (presets3d.ts:17)
   m->hold_time = 1.5;
-  m->target_volume = 400e-6;
+  m->target_volume = 400 * 1e-6;  // 400 * ML, evaluated as the reference does
   m->anticipation = 0.254;
   m->repeats = 1;
   m->repeat_gap = 1.5;
@@ -192,6 +226,7 @@ void pl_gentle_pour(double cell_mm, double seconds, pl_config* c) {
   c->duration = seconds;
   c->preconditioner = PL_PRECOND_MIC0;
   c->solve_precision = PL_SOLVE_F64;
+  c->device = -1;
 }
 
 int pl_create(const pl_config* cfg, pl_sim** out) {
@@ -208,11 +243,18 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   for (int k = 0; k < 3; k++) s->band_counts[k] = init.band_counts[k];
   s->origin = init.origin;
   const Geo& g = s->g;
-  cudaGetDevice(&s->device);
-  cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  cudaError_t e = cudaSuccess;
+  if (cfg->device >= 0)
+    e = cudaSetDevice(cfg->device);
+  else
+    e = cudaGetDevice(&s->device);
+  if (cfg->device >= 0) s->device = cfg->device;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->pinned, sizeof(SimScalars), cudaHostAllocDefault);
+  for (int i = 0; i <= PL_STAGES && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
   if (e != cudaSuccess) {
-    delete s;
-    return fail(PL_E_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    pl_destroy(s);
+    return fail(PL_E_CUDA, "pl_create: stream, events or pinned staging: %s", cudaGetErrorString(e));
   }
   // one allocation for everything
   const size_t N = g.n, C = g.nc, F = g.nf, B = g.nbins + 1;
@@ -234,8 +276,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   for (size_t b : sizes) total += al256(b);
   e = cudaMalloc(&s->mem, total);
   if (e != cudaSuccess) {
-    cudaStreamDestroy(s->st);
-    delete s;
+    pl_destroy(s);
     return fail(PL_E_NOMEM, "cudaMalloc(%zu): %s", total, cudaGetErrorString(e));
   }
   s->mem_bytes = total;
@@ -306,14 +347,76 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   return PL_OK;
 }
 
+int pl_plan(const pl_config* cfg, pl_sizes* o, double* x, double* y, double* z, uint8_t* origin) {
+  if (!cfg || !o) return fail(PL_E_ARG, "pl_plan: null argument");
+  char err[256] = "";
+  HostInit init;
+  int rc = host_construct(*cfg, &init, err, sizeof err);
+  if (rc) return fail(rc, "%s", err);
+  const Geo& g = init.geo;
+  std::memset(o, 0, sizeof *o);
+  o->n = g.n;
+  o->nx = g.nx;
+  o->ny = g.ny;
+  o->nz = g.nz;
+  o->h = g.h;
+  o->parcel_volume = g.parcel_volume;
+  o->pivot_world[0] = g.pwx;
+  o->pivot_world[1] = g.pwy;
+  o->fill_height = init.fill_height;
+  for (int k = 0; k < 3; k++) o->band_counts[k] = init.band_counts[k];
+  const size_t n = size_t(g.n);
+  if (x) std::memcpy(x, init.x.data(), n * 8);
+  if (y) std::memcpy(y, init.y.data(), n * 8);
+  if (z) std::memcpy(z, init.z.data(), n * 8);
+  if (origin) std::memcpy(origin, init.origin.data(), n);
+  return PL_OK;
+}
+
 void pl_destroy(pl_sim* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->mem) cudaFree(s->mem);
+  for (int i = 0; i <= PL_STAGES; i++)
+    if (s->ev[i]) cudaEventDestroy(s->ev[i]);
+  if (s->pinned) cudaFreeHost(s->pinned);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
+}
+
+int pl_enqueue_substeps(pl_sim* s, int32_t count) {
+  if (!s || count < 0) return fail(PL_E_ARG, "pl_enqueue_substeps: bad argument");
+  cudaSetDevice(s->device);
+  s->hs.end_time = INFINITY;  // run until finished
+  s->hs.force_step = 0;
+  std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
+  // only the control fields change: copy end_time .. forced_dt
+  const size_t off = offsetof(SimScalars, end_time);
+  const size_t len = offsetof(SimScalars, active) - off;
+  CK(cudaMemcpyAsync((char*)s->P.sc + off, (char*)s->pinned + off, len, cudaMemcpyHostToDevice, s->st));
+  for (int i = 0; i < count; i++) CK(cudaGraphLaunch(s->exec, s->st));
+  s->pending = 1;
+  return PL_OK;
+}
+
+void* pl_stream(const pl_sim* s) { return s ? (void*)s->st : nullptr; }
+
+int pl_enable_stage_timing(pl_sim* s, int32_t on) {
+  if (!s) return fail(PL_E_ARG, "pl_enable_stage_timing: null handle");
+  cudaSetDevice(s->device);
+  CK(cudaStreamSynchronize(s->st));
+  s->timing = on ? 1 : 0;
+  return build_graph(s);
+}
+
+int pl_stage_times(pl_sim* s, float ms[PL_STAGES]) {
+  if (!s || !ms) return fail(PL_E_ARG, "pl_stage_times: null argument");
+  if (!s->timing) return fail(PL_E_STATE, "pl_stage_times: stage timing is off");
+  CK(cudaStreamSynchronize(s->st));
+  for (int i = 0; i < PL_STAGES; i++) CK(cudaEventElapsedTime(&ms[i], s->ev[i], s->ev[i + 1]));
+  return PL_OK;
 }
 
 int pl_get_sizes(const pl_sim* s, pl_sizes* o) {
@@ -334,6 +437,8 @@ int pl_get_sizes(const pl_sim* s, pl_sizes* o) {
 
 int pl_stable_dt(pl_sim* s, double* out) {
   if (!s || !out) return fail(PL_E_ARG, "pl_stable_dt: null argument");
+  int rc = settle(s);
+  if (rc) return rc;
   *out = host_stable_dt(s);
   return PL_OK;
 }
@@ -343,9 +448,11 @@ int pl_finished(const pl_sim* s) { return s && host_finished(s) ? 1 : 0; }
 int pl_step(pl_sim* s, double dt) {
   if (!s) return fail(PL_E_ARG, "pl_step: null handle");
   cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
   s->hs.force_step = 1;
   s->hs.forced_dt = dt > 0 ? dt : 0;
-  int rc = push_scalars(s);
+  rc = push_scalars(s);
   if (rc) return rc;
   CK(cudaGraphLaunch(s->exec, s->st));
   return pull_scalars(s);
@@ -354,10 +461,12 @@ int pl_step(pl_sim* s, double dt) {
 int pl_advance(pl_sim* s, double duration, pl_diagnostics* out) {
   if (!s) return fail(PL_E_ARG, "pl_advance: null handle");
   cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
   const double end = s->hs.time + duration;  // solver3d.ts:282
   s->hs.end_time = end;
   s->hs.force_step = 0;
-  int rc = push_scalars(s);
+  rc = push_scalars(s);
   if (rc) return rc;
   for (int guard = 0; guard < 1000000; guard++) {
     if (!(s->hs.time < end - 1e-12 && !host_finished(s))) break;
@@ -381,6 +490,8 @@ int pl_sync(pl_sim* s) {
 int pl_set_tilt_target(pl_sim* s, double angle_deg, double time) {  // motion.ts:40-44
   if (!s) return fail(PL_E_ARG, "pl_set_tilt_target: null handle");
   (void)time;
+  int rc = settle(s);
+  if (rc) return rc;
   double a = std::max(0.0, std::min(s->hs.motion.max_angle_deg, angle_deg));
   s->hs.ctl.target = a * DEG;
   return push_scalars(s);
@@ -395,6 +506,8 @@ int pl_controller(const pl_sim* s, double* angle_deg, int32_t* phase) {
 
 int pl_get_diagnostics(pl_sim* s, pl_diagnostics* d) {  // solver3d.ts:796-814
   if (!s || !d) return fail(PL_E_ARG, "pl_get_diagnostics: null argument");
+  int rc = settle(s);
+  if (rc) return rc;
   const SimScalars& h = s->hs;
   const double v = s->g.parcel_volume * 2 * 1e6;
   std::memset(d, 0, sizeof *d);
@@ -417,11 +530,14 @@ int pl_get_diagnostics(pl_sim* s, pl_diagnostics* d) {  // solver3d.ts:796-814
   std::memcpy(&md, &h.max_div_bits, 8);
   d->max_divergence = md / s->g.h;
   d->interior_density = h.interior;
+  d->liquid_cells = h.m;
   return PL_OK;
 }
 
 int pl_discharged_fractions(pl_sim* s, double out[3]) {  // solver3d.ts:817-823
   if (!s || !out) return fail(PL_E_ARG, "pl_discharged_fractions: null argument");
+  int rc = settle(s);
+  if (rc) return rc;
   const int* c = s->hs.by_origin;
   int n = c[0] + c[1] + c[2];
   if (n == 0) return PL_NONE;
@@ -496,6 +612,8 @@ int pl_read_render_positions(pl_sim* s, float* xyz6n) {
 
 int pl_get_state(pl_sim* s, pl_sim_state* st) {
   if (!s || !st) return fail(PL_E_ARG, "pl_get_state: null argument");
+  int rc = settle(s);
+  if (rc) return rc;
   const SimScalars& h = s->hs;
   std::memset(st, 0, sizeof *st);
   st->time = h.time;
@@ -520,6 +638,8 @@ int pl_set_state(pl_sim* s, const pl_sim_state* st, const double* x, const doubl
                  const double* vx, const double* vy, const double* vz, const uint8_t* status) {
   if (!s) return fail(PL_E_ARG, "pl_set_state: null handle");
   cudaSetDevice(s->device);
+  int rc0 = settle(s);
+  if (rc0) return rc0;
   SimScalars& h = s->hs;
   const int n = s->g.n;
   if (x && y && z && status) {

@@ -757,22 +757,28 @@ __global__ void k_export_correction(Geo g, DevPtrs P, float* out) {
 
 static inline int blocks(int n, int t) { return (n + t - 1) / t; }
 
-void launch_substep_front(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_controller<<<1, 1, 0, st>>>(g, P);
   k_bin_count<<<blocks(max(g.n, SCAN_MAX_TILES), 256), 256, 0, st>>>(g, P);
   k_scan_classify<<<blocks(g.nbins, SCAN_TILE), SCAN_THREADS, 0, st>>>(g, P);
   k_bin_place<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
   k_bin_permute<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
+}
+
+void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
 }
 
-void launch_substep_middle(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+void launch_stage_extrap(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_grad_ext1<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
   k_ext2<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
+}
+
+void launch_stage_density(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_density<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P);
 }
 
-void launch_substep_back(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+void launch_stage_advect(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_advect<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
 }
 

@@ -26,8 +26,10 @@ EXPORTED = [
     "pl_get_sizes", "pl_stable_dt", "pl_finished", "pl_step", "pl_advance", "pl_sync", "pl_set_tilt_target",
     "pl_controller", "pl_get_diagnostics", "pl_discharged_fractions", "pl_read_particles",
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
-    "pl_get_field", "pl_pcg_solve_device",
+    "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
+    "pl_stage_times", "pl_plan",
 ]
+STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
 
 class EngineError(RuntimeError):
@@ -79,6 +81,12 @@ def lib() -> C.CDLL:
     L.pl_get_field.argtypes = [P, C.c_int32, P, C.c_size_t]
     L.pl_pcg_solve_device.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                       C.c_int32, P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp]
+    L.pl_plan.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Sizes), dp, dp, dp, u8p]
+    L.pl_enqueue_substeps.argtypes = [P, C.c_int32]
+    L.pl_stream.argtypes = [P]
+    L.pl_stream.restype = C.c_void_p
+    L.pl_enable_stage_timing.argtypes = [P, C.c_int32]
+    L.pl_stage_times.argtypes = [P, fp]
     _lib = L
     return L
 
@@ -96,6 +104,19 @@ def _ptr(a: np.ndarray, t):
 def gentle_pour(cell_mm: float, seconds: float, **over) -> abi.Config:
     """gentlePour3D(cellMm, seconds) (src/sim3d/presets3d.ts:9-26) with keyword overrides."""
     return abi.gentle_pour(cell_mm, seconds, **over)
+
+
+def plan(cfg: abi.Config) -> dict:
+    """Host part of the constructor without a device (pl_plan): sizes, seeded parcels, origins."""
+    L = lib()
+    s = abi.Sizes()
+    _check(L.pl_plan(C.byref(cfg), C.byref(s), None, None, None, None))
+    n = s.n
+    x, y, z = np.zeros(n), np.zeros(n), np.zeros(n)
+    o = np.zeros(n, np.uint8)
+    _check(L.pl_plan(C.byref(cfg), C.byref(s), _ptr(x, C.c_double), _ptr(y, C.c_double), _ptr(z, C.c_double),
+                     _ptr(o, C.c_uint8)))
+    return {"sizes": s, "x": x, "y": y, "z": z, "origin": o}
 
 
 class Simulation3D:
@@ -174,6 +195,24 @@ class Simulation3D:
 
     def sync(self):
         _check(lib().pl_sync(self._h))
+
+    def enqueue(self, count: int = 1):
+        """Queue `count` stable substeps without waiting (pl_enqueue_substeps)."""
+        _check(lib().pl_enqueue_substeps(self._h, count))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this simulation (for ordering external work such as timing events)."""
+        return lib().pl_stream(self._h) or 0
+
+    def enable_stage_timing(self, on: bool = True):
+        _check(lib().pl_enable_stage_timing(self._h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        """Device milliseconds per stage of the last completed substep."""
+        out = np.zeros(len(STAGES), np.float32)
+        _check(lib().pl_stage_times(self._h, _ptr(out, C.c_float)))
+        return dict(zip(STAGES, out.tolist()))
 
     # ------------------------------------------------------------ controller
     def set_target(self, angle_deg: float, time: float | None = None):
