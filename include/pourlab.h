@@ -57,8 +57,10 @@ enum pl_phase {
 
 /* Pressure preconditioner. MIC0 is the reference's MIC(0) (solver3d.ts:883-900, 955-973),
  * applied in wavefront order on the device; MG is a 3D geometric multigrid V-cycle (the 3D form
- * of src/sim/multigrid.ts with a red-black Gauss-Seidel smoother). */
-enum pl_preconditioner { PL_PRECOND_MIC0 = 0, PL_PRECOND_MG = 1 };
+ * of src/sim/multigrid.ts with a red-black Gauss-Seidel smoother); CHEB is the Chebyshev
+ * polynomial of the WebGPU port (src/gpu3d/shaders.ts:588-622). MG and CHEB run on one
+ * 16-CTA thread-block cluster with the vectors in distributed shared memory. */
+enum pl_preconditioner { PL_PRECOND_MIC0 = 0, PL_PRECOND_MG = 1, PL_PRECOND_CHEB = 2 };
 /* Arithmetic of the pressure solves: F64 keeps every solver vector in FP64; MIXED keeps the
  * Krylov and smoother vectors in FP32 with FP64 inner products, an FP64 solution and FP64
  * iterative refinement of the true residual. */
@@ -113,7 +115,9 @@ typedef struct pl_config {
   int32_t preconditioner;  /* enum pl_preconditioner */
   int32_t solve_precision; /* enum pl_solve_precision */
   int32_t device;          /* CUDA device ordinal; -1 = the calling thread's current device */
-  int32_t reserved[5];
+  int32_t solve_cluster;   /* CTAs of the cluster solves (1-16; 0 = 16), see pl_autotune_solver */
+  int32_t solve_threads;   /* threads per CTA of the cluster solves (32-512; 0 = 256) */
+  int32_t reserved[3];
 } pl_config;
 
 /* Diagnostics3D (src/sim3d/solver3d.ts:45-60). */
@@ -265,6 +269,14 @@ enum pl_stage {
 int pl_enable_stage_timing(pl_sim* sim, int32_t on);
 /* Device milliseconds per stage of the last completed substep (needs stage timing on). */
 int pl_stage_times(pl_sim* sim, float ms[PL_STAGES]);
+/* Launch-shape tuner of the cluster solves (no counterpart in the reference): runs `substeps`
+ * substeps of cfg from its initial state for every candidate (cluster CTAs x threads per CTA) on a
+ * scratch simulation and returns the shape with the smallest pressure + correction time, and that
+ * time per substep. Set the result in pl_config.solve_cluster / solve_threads: results depend on
+ * the shape only through the order of inner-product sums, so a fixed shape keeps runs bitwise
+ * reproducible. */
+int pl_autotune_solver(const pl_config* cfg, int32_t substeps, int32_t* best_cluster, int32_t* best_threads,
+                       float* best_ms);
 
 /* ------------------------------------------------------------------ controller */
 

@@ -22,7 +22,7 @@ MOTION_STILL, MOTION_POUR, MOTION_TILT, MOTION_MANUAL = 0, 1, 2, 3
 MOTION_KINDS = {"still": MOTION_STILL, "pour": MOTION_POUR, "tilt": MOTION_TILT, "manual": MOTION_MANUAL}
 PHASES = ["wait", "tilt-in", "hold", "return", "rest", "done", "manual"]
 
-PRECOND_MIC0, PRECOND_MG = 0, 1
+PRECOND_MIC0, PRECOND_MG, PRECOND_CHEB = 0, 1, 2
 SOLVE_F64, SOLVE_MIXED = 0, 1
 
 FIELD_CELL = 0
@@ -87,7 +87,9 @@ class Config(C.Structure):
         ("preconditioner", C.c_int32),
         ("solve_precision", C.c_int32),
         ("device", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("solve_cluster", C.c_int32),
+        ("solve_threads", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

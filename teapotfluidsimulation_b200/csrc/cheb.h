@@ -1,0 +1,33 @@
+// Chebyshev-preconditioned CG on one thread-block cluster (see cheb.cu).
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace pl {
+
+constexpr int CHEB_CLUSTER = 16;       // largest cluster (non-portable size, one CTA per SM)
+constexpr int CHEB_MAX_THREADS = 512;  // largest CTA
+constexpr int CHEB_SMEM = 224 * 1024;  // dynamic shared memory per CTA
+constexpr int CHEB_DEGREE = 12;        // polynomial degree (stencil applications per CG iteration)
+constexpr double CHEB_LO = 0.03;        // lower end of the D^-1 A interval the polynomial targets
+constexpr int PULL_UNROLL = 8;         // halo slots whose DSMEM loads one thread keeps in flight
+
+struct ChebArgs {
+  const double* b;  // list-indexed rhs
+  double* q;        // list-indexed solution
+  double tol;
+  int max_iter;
+  int is_correction;
+  int mixed;
+  int degree;
+  double cheb_lo;
+  int cluster;     // CTAs in the cluster (launch shape, chosen by the tuner)
+  int threads;     // threads per CTA
+  int smem_bytes;  // dynamic shared memory per CTA
+};
+
+void cheb_configure();
+void launch_cheb_solve(const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st);
+
+}  // namespace pl

@@ -49,6 +49,8 @@ struct Geo {
   int max_iter;
   int precond;
   int precision;
+  int solve_cluster;  // launch shape of the cluster solves (set by the tuner)
+  int solve_threads;
   double parcel_volume;
   double R;  // Math.hypot(nx, ny) * h  (solver3d.ts:275)
   // teapot
@@ -90,6 +92,8 @@ struct SimScalars {
   int errors;    // ERR_* bits
   int outliers;  // in-pot parcels outside the interior cells (clamped into it)
   int corr_any;  // density rhs has a non-zero entry
+  int mg_status;  // 1: the cluster multigrid solve ran; 0: the wavefront solver must run
+  int pad2;
   unsigned long long max_speed_bits;  // max |v|^2 (FP64 bits) of in-pot parcels after advect
   unsigned long long max_div_bits;    // max |div| (FP64 bits) after projection
   double interior;                    // mean interior density ratio
@@ -249,6 +253,7 @@ struct DevPtrs {
   // solver scratch (list-indexed)
   void* solver_ws;
   size_t solver_ws_bytes;
+  void* mg_ws;  // multigrid hierarchy
   // render
   float* render;
   SimScalars* sc;

@@ -14,7 +14,9 @@
 #include <vector>
 
 #include "common.cuh"
+#include "cheb.h"
 #include "kernels.h"
+#include "mg.h"
 #include "setup.h"
 
 using namespace pl;
@@ -271,6 +273,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       solver_ws_bytes(int(C)),                         // solver
       N * 6 * 4,                                       // render
       sizeof(SimScalars), F * 4,                       // scalars, export
+      mg_ws_bytes(g, nullptr),                         // multigrid hierarchy
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -320,6 +323,9 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.render = (float*)take();
   P.sc = (SimScalars*)take();
   s->export_buf = (float*)take();
+  P.mg_ws = take();
+  mg_configure();
+  cheb_configure();
   int nn = g.n;
   cudaMemcpyAsync(P.start + g.nbins, &nn, 4, cudaMemcpyHostToDevice, s->st);
   // initial scalars
@@ -402,6 +408,50 @@ int pl_enqueue_substeps(pl_sim* s, int32_t count) {
 }
 
 void* pl_stream(const pl_sim* s) { return s ? (void*)s->st : nullptr; }
+
+int pl_autotune_solver(const pl_config* cfg, int32_t substeps, int32_t* best_cluster, int32_t* best_threads,
+                       float* best_ms) {
+  if (!cfg || substeps < 1 || !best_cluster || !best_threads) return fail(PL_E_ARG, "pl_autotune_solver: bad argument");
+  pl_config c = *cfg;
+  c.preconditioner = PL_PRECOND_CHEB;
+  const int clusters[] = {16, 8, 12, 4};
+  const int threads[] = {256, 128, 512};
+  float best = INFINITY;
+  int bc = 0, bt = 0;
+  for (int ci : clusters)
+    for (int ti : threads) {
+      c.solve_cluster = ci;
+      c.solve_threads = ti;
+      pl_sim* s = nullptr;
+      if (pl_create(&c, &s) != PL_OK) {
+        cudaGetLastError();
+        continue;
+      }
+      int rc = pl_enable_stage_timing(s, 1);
+      float tot = 0;
+      for (int k = 0; k < substeps + 1 && rc == PL_OK; k++) {
+        rc = pl_step(s, -1.0);
+        float ms[PL_STAGES];
+        if (rc == PL_OK) rc = pl_stage_times(s, ms);
+        if (rc == PL_OK && k > 0) tot += ms[PL_STAGE_PRESSURE] + ms[PL_STAGE_CORRECTION];  // first one warms up
+      }
+      const bool ran = rc == PL_OK && s->hs.mg_status == 1;  // the cluster solve (not the fallback) ran
+      pl_destroy(s);
+      cudaGetLastError();
+      if (!ran) continue;
+      tot /= substeps;
+      if (tot < best) {
+        best = tot;
+        bc = ci;
+        bt = ti;
+      }
+    }
+  if (bc == 0) return fail(PL_E_STATE, "pl_autotune_solver: no launch shape ran");
+  *best_cluster = bc;
+  *best_threads = bt;
+  if (best_ms) *best_ms = best;
+  return PL_OK;
+}
 
 int pl_enable_stage_timing(pl_sim* s, int32_t on) {
   if (!s) return fail(PL_E_ARG, "pl_enable_stage_timing: null handle");

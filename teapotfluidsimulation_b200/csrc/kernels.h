@@ -34,6 +34,7 @@ struct SolveArgs {
   int max_iter;
   int is_correction;  // density solve: gated by corr_any, records corr_iters and the interior mean
   int factor;         // build the wavefront order and the MIC(0) factor first
+  int fallback;       // run only when the cluster multigrid solve did not (mg_status == 0)
 };
 
 SolverWs solver_ws_carve(void* base, int cap);

@@ -13,6 +13,8 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "cheb.h"
+#include "mg.h"
 
 namespace pl {
 
@@ -360,6 +362,7 @@ __device__ SolveOut pcg_block(const SolverWs& W, int m, const double* b, double*
 __global__ void __launch_bounds__(SOLVER_THREADS) k_pcg(Geo g, DevPtrs P, SolverWs W, SolveArgs a) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
+  if (a.fallback && sc->mg_status) return;  // the cluster multigrid solve already ran
   __shared__ double s_red[64];
   __shared__ int s_lstart[MAX_LEVELS + 1];
   __shared__ int s_hist[MAX_LEVELS + 1];
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(SOLVER_THREADS) k_pcg(Geo g, DevPtrs P, Solver
       return;
     }
   }
-  SolveOut o = pcg_block(W, m, a.b, a.q, a.tol, a.max_iter, a.factor != 0, red, s_lstart, s_hist);
+  SolveOut o = pcg_block(W, m, a.b, a.q, a.tol, a.max_iter, a.factor != 0 || a.fallback != 0, red, s_lstart, s_hist);
   if (threadIdx.x == 0) {
     if (o.iterations < 0) {
       atomicOr(&sc->errors, ERR_SOLVER_SIZE);
@@ -400,16 +403,40 @@ __global__ void __launch_bounds__(SOLVER_THREADS) k_pcg(Geo g, DevPtrs P, Solver
 
 static SolverWs ws_of(const DevPtrs& P, int cap) { return solver_ws_carve(P.solver_ws, cap); }
 
+// Pressure solve (project(), solver3d.ts:530-543). With the multigrid preconditioner the cluster
+// solve runs first and the wavefront MIC(0) solve only if the cluster's shared memory could not
+// hold the hierarchy (it then factors as usual).
 void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   SolverWs W = ws_of(P, g.nc);
   k_solve_setup<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, W, 1);
-  SolveArgs a{W.bp, P.q, g.tol, g.max_iter, 0, 1};
+  const bool mg = g.precond == PL_PRECOND_MG, cheb = g.precond == PL_PRECOND_CHEB;
+  if (mg) {
+    MgWs M = mg_ws_carve(g, P.mg_ws, P, W);
+    launch_mg_setup(g, P, M, st);
+    launch_mg_solve(g, P, M, MgArgs{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED}, st);
+  } else if (cheb) {
+    launch_cheb_solve(g, P, W,
+                      ChebArgs{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
+                               g.solve_cluster, g.solve_threads, CHEB_SMEM},
+                      st);
+  }
+  SolveArgs a{W.bp, P.q, g.tol, g.max_iter, 0, 1, (mg || cheb) ? 1 : 0};
   k_pcg<<<1, SOLVER_THREADS, 0, st>>>(g, P, W, a);
 }
 
+// Density-correction solve (solver3d.ts:671-674): tolerance 1e-4, at most 80 iterations.
 void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   SolverWs W = ws_of(P, g.nc);
-  SolveArgs a{P.rhs, P.qc, 1e-4, 80, 1, 0};  // solver3d.ts:673
+  const bool mg = g.precond == PL_PRECOND_MG, cheb = g.precond == PL_PRECOND_CHEB;
+  if (mg) {
+    MgWs M = mg_ws_carve(g, P.mg_ws, P, W);
+    launch_mg_solve(g, P, M, MgArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED}, st);
+  } else if (cheb) {
+    launch_cheb_solve(g, P, W, ChebArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
+                               g.solve_cluster, g.solve_threads, CHEB_SMEM},
+                      st);
+  }
+  SolveArgs a{P.rhs, P.qc, 1e-4, 80, 1, 0, (mg || cheb) ? 1 : 0};
   k_pcg<<<1, SOLVER_THREADS, 0, st>>>(g, P, W, a);
 }
 

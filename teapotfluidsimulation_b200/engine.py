@@ -27,7 +27,7 @@ EXPORTED = [
     "pl_controller", "pl_get_diagnostics", "pl_discharged_fractions", "pl_read_particles",
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
     "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
-    "pl_stage_times", "pl_plan",
+    "pl_stage_times", "pl_plan", "pl_autotune_solver",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
     L.pl_pcg_solve_device.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                       C.c_int32, P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp]
     L.pl_plan.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Sizes), dp, dp, dp, u8p]
+    L.pl_autotune_solver.argtypes = [C.POINTER(abi.Config), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_float)]
     L.pl_enqueue_substeps.argtypes = [P, C.c_int32]
     L.pl_stream.argtypes = [P]
     L.pl_stream.restype = C.c_void_p
@@ -117,6 +119,13 @@ def plan(cfg: abi.Config) -> dict:
     _check(L.pl_plan(C.byref(cfg), C.byref(s), _ptr(x, C.c_double), _ptr(y, C.c_double), _ptr(z, C.c_double),
                      _ptr(o, C.c_uint8)))
     return {"sizes": s, "x": x, "y": y, "z": z, "origin": o}
+
+
+def autotune_solver(cfg: abi.Config, substeps: int = 3) -> tuple[int, int, float]:
+    """pl_autotune_solver: (cluster CTAs, threads per CTA, ms per substep) of the fastest shape."""
+    c, t, ms = C.c_int32(), C.c_int32(), C.c_float()
+    _check(lib().pl_autotune_solver(C.byref(cfg), substeps, C.byref(c), C.byref(t), C.byref(ms)))
+    return c.value, t.value, ms.value
 
 
 class Simulation3D:
