@@ -31,8 +31,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "gentle 400 mL pour, 4 mm cells, half pot (81x81x22 grid, 88,856 parcels), seed 1"
-KERNELS_PER_SUBSTEP = 13  # controller, bin count/scan/place/permute, p2g, solve setup, pcg, 2x extrapolation,
-#                           density, correction pcg, advect
+# kernels per substep: controller, bin count/scan/place/permute, p2g, solve setup, pressure solve,
+# 2x extrapolation, density, correction solve, advect; the cluster solves add their gated fallback
+KERNELS_PER_SUBSTEP = {"mic0": 13, "cheb": 15, "mg": 16}
 
 
 def parse():
@@ -42,7 +43,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cell-mm", type=float, default=4.0)
-    ap.add_argument("--precond", default="mic0", choices=["mic0", "mg"])
+    ap.add_argument("--precond", default="cheb", choices=["mic0", "mg", "cheb"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     ap.add_argument("--start", type=float, default=0.0, help="simulated seconds to advance before warm-up")
     ap.add_argument("--cpu-sample", type=int, default=60, help="substeps of the CPU baseline sample")
     return ap.parse_args()
@@ -52,7 +54,8 @@ def make_cfg(args):
     from teapotfluidsimulation_b200 import abi
 
     cfg = abi.gentle_pour(args.cell_mm, 20.0)
-    cfg.preconditioner = abi.PRECOND_MG if args.precond == "mg" else abi.PRECOND_MIC0
+    cfg.preconditioner = {"mic0": abi.PRECOND_MIC0, "mg": abi.PRECOND_MG, "cheb": abi.PRECOND_CHEB}[args.precond]
+    cfg.solve_precision = abi.SOLVE_MIXED if args.precision == "mixed" else abi.SOLVE_F64
     return cfg
 
 
@@ -177,15 +180,22 @@ def profile_traffic():
     return None
 
 
-def pcg_bytes_per_iteration(m: int) -> float:
-    """Algorithmic bytes of one FP64 MIC(0)-PCG iteration over m liquid cells.
+def pcg_bytes_per_iteration(m: int, precond: str, precision: str) -> float:
+    """Algorithmic bytes of one PCG iteration over m liquid cells, each array counted once per pass.
 
-    Each array counted once per logical pass: apply A (s, 6 neighbour indices, diagonal, write As:
-    8+24+8+8), s.As (16), q/r update (read q, s, r, As, write q, r: 48), the two MIC(0) sweeps
-    (r or qv, pc, 3 neighbour indices, 3 neighbour values, write: 2 x 48), z.r (16), direction
-    update (read z, s, write s: 24). Total 248 bytes per liquid cell.
+    MIC(0) in FP64: apply A (s, 6 neighbour indices, diagonal, write As: 8+24+8+8), s.As (16),
+    q/r update (read q, s, r, As, write q, r: 48), the two MIC(0) sweeps (r or qv, pc, 3 neighbour
+    indices, 3 neighbour values, write: 2 x 48), z.r (16), direction update (24): 248 B per cell.
+    Chebyshev (degree 12) with vectors of w bytes: s and A s formed from z and the old s
+    (z, s, 6 u16 indices, diagonal, write s and As: 4w+12+4), q/r update (q 16, s, r r/w, As: 4w+16),
+    and per Chebyshev step the direction (read + write), residual (read + write), z (read + write),
+    inverse diagonal, diagonal and indices (7w+16), plus z.r and max|r| (2w).
     """
-    return 248.0 * m
+    if precond == "mic0":
+        return 248.0 * m
+    w = 4.0 if precision == "mixed" else 8.0
+    deg = 12
+    return m * ((4 * w + 16) + (4 * w + 16) + deg * (7 * w + 16) + 2 * w)
 
 
 def run_cpu_baseline(args, substeps: int) -> dict:
@@ -289,7 +299,7 @@ def run_ours(args):
         steps_done += 1
         d = sim.diagnostics()
         iters.append(d["pressureIterations"])
-        pcg_work += pcg_bytes_per_iteration(d["liquidCells"]) * d["pressureIterations"]
+        pcg_work += pcg_bytes_per_iteration(d["liquidCells"], args.precond, args.precision) * d["pressureIterations"]
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()
@@ -327,15 +337,18 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": max_ms / max(steps_done, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve / f32 parcels and faces", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "preconditioner": args.precond,
+                   "solve_precision": args.precision,
                    "start_s": args.start, "simulated_s": sim_s, "l2": "256 MiB buffer written between substeps",
                    "parallelism": f"replicas x{world}"},
         "pressure_ms_per_substep": pres_ms,
         "pressure_iterations_mean": (sum(iters) / len(iters)) if iters else 0,
         "stages_ms_per_substep": {k: v / max(steps_done, 1) for k, v in stage_acc.items()},
-        "gpu_launches": KERNELS_PER_SUBSTEP * steps_done,
+        "gpu_launches": KERNELS_PER_SUBSTEP[args.precond] * steps_done,
         "e2e": {"value": e2e_value, "unit": "sim-s/wall-s", "h2d_bytes_per_step": scalars,
                 "d2h_bytes_per_step": scalars},
-        "roofline": {"kernel": "k_pcg (pressure solve, with its setup)", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": "pressure solve stage (k_solve_setup + %s)" % (
+                         "k_pcg" if args.precond == "mic0" else "k_chebpcg" if args.precond == "cheb" else "k_mgpcg"),
+                     "bound": "hbm", "achieved": achieved,
                      "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                      "frac": achieved / peaks.get("hbm_gbs", 1.0), "peak_kind": peak_kind,
                      "traffic": traffic},

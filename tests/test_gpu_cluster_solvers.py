@@ -1,0 +1,101 @@
+"""The thread-block-cluster pressure solves (Chebyshev-PCG and multigrid-PCG) against the oracle.
+
+The oracle solves with the reference's MIC(0)-PCG; a different preconditioner converges to the same
+solution within the solve tolerance, so the fields are compared at a tight tolerance (1e-10 max-norm
+residual on both sides), where relative L2 < 1e-5 leaves no room for a wrong operator, rhs or
+boundary condition. Whole pours are compared with the reference's committed results.
+"""
+import numpy as np
+import pytest
+
+from teapotfluidsimulation_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def one_step(engine, oracle_mod, mm, precond, precision, tol):
+    cfg = abi.gentle_pour(mm, 20, pressure_tolerance=tol)
+    cpu = oracle_mod.OracleSim(cfg)
+    cfg.preconditioner = precond
+    cfg.solve_precision = precision
+    gpu = engine.Simulation3D(cfg)
+    for _ in range(2):
+        dt = cpu.stable_dt()
+        cpu.step(dt)
+        gpu.step(dt)
+    return gpu, cpu
+
+
+@pytest.mark.parametrize("precond,precision", [(abi.PRECOND_CHEB, abi.SOLVE_F64), (abi.PRECOND_CHEB, abi.SOLVE_MIXED),
+                                               (abi.PRECOND_MG, abi.SOLVE_F64)])
+@pytest.mark.parametrize("mm", [5, 4])
+def test_fields_match_oracle(engine, oracle_mod, mm, precond, precision):
+    gpu, cpu = one_step(engine, oracle_mod, mm, precond, precision, 1e-10)
+    assert np.array_equal(gpu.field(abi.FIELD_CELL), cpu.field(abi.FIELD_CELL))
+    for f in (abi.FIELD_PRESSURE, abi.FIELD_VELOCITY, abi.FIELD_VELOCITY_PREV):
+        assert rel_l2(gpu.field(f), cpu.field(f)) < 1e-5, f
+    d = gpu.diagnostics()
+    assert d["pressureFailures"] == 0 and d["pressureIterations"] > 0
+    gpu.destroy()
+
+
+def test_default_tolerance_residual(engine, oracle_mod):
+    # at the reference tolerance (1e-6) the solution differs from MIC(0)'s only within that tolerance
+    gpu, cpu = one_step(engine, oracle_mod, 4, abi.PRECOND_CHEB, abi.SOLVE_F64, 1e-6)
+    assert rel_l2(gpu.field(abi.FIELD_PRESSURE), cpu.field(abi.FIELD_PRESSURE)) < 1e-4
+    assert rel_l2(gpu.field(abi.FIELD_VELOCITY), cpu.field(abi.FIELD_VELOCITY)) < 1e-5
+    assert gpu.diagnostics()["pressureIterations"] < cpu.diagnostics()["pressureIterations"]
+    gpu.destroy()
+
+
+def test_standalone_and_engine_agree_on_rerun(engine):
+    # two simulations with the same config are bitwise identical (deterministic reductions)
+    cfg = abi.gentle_pour(5, 20)
+    cfg.preconditioner = abi.PRECOND_CHEB
+    a, b = engine.Simulation3D(cfg), engine.Simulation3D(cfg)
+    a.advance(0.5)
+    b.advance(0.25)
+    b.advance(0.25)
+    pa, pb = a.particles(), b.particles()
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(pa[k], pb[k]), k
+    a.destroy()
+    b.destroy()
+
+
+def test_autotune_returns_a_working_shape(engine):
+    cfg = abi.gentle_pour(10, 20)
+    c, t, ms = engine.engine.autotune_solver(cfg, 2)
+    assert 1 <= c <= 16 and t in (128, 256, 512) and ms > 0
+    cfg.preconditioner = abi.PRECOND_CHEB
+    cfg.solve_cluster, cfg.solve_threads = c, t
+    sim = engine.Simulation3D(cfg)
+    sim.step(-1.0)
+    assert sim.diagnostics()["pressureFailures"] == 0
+    sim.destroy()
+
+
+@pytest.mark.slow
+def test_whole_pour_4mm_against_reference(engine, goldens):
+    # benchmarks/run3d.json 4 mm: 410.54 mL, shares 29.22 / 50.96 / 19.82 %
+    ref = {r["cellMm"]: r for r in goldens["run3d"]}[4]
+    cfg = abi.gentle_pour(4, 20)
+    cfg.preconditioner = abi.PRECOND_CHEB
+    sim = engine.Simulation3D(cfg)
+    done_at = -1.0
+    while not sim.finished:  # benchmarks/run3d.ts:14-23
+        d = sim.advance(0.5)
+        if d["phase"] == "done" and done_at < 0:
+            done_at = d["time"]
+        if done_at >= 0 and d["time"] > done_at + 1.5:
+            break
+    d = sim.diagnostics()
+    sh = sim.discharged_fractions()
+    assert abs(d["dischargedMl"] / ref["dischargedMl"] - 1) < 0.003, d["dischargedMl"]
+    assert np.abs(sh - np.array(ref["dischargedFractions"])).max() < 0.013, sh
+    assert d["spilledMl"] == 0 and d["lostMl"] == 0 and d["pressureFailures"] == 0
+    sim.destroy()
