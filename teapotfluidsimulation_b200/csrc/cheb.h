@@ -11,7 +11,7 @@ constexpr int CHEB_MAX_THREADS = 512;  // largest CTA
 constexpr int CHEB_SMEM = 224 * 1024;  // dynamic shared memory per CTA
 constexpr int CHEB_DEGREE = 12;        // polynomial degree (stencil applications per CG iteration)
 constexpr double CHEB_LO = 0.03;        // lower end of the D^-1 A interval the polynomial targets
-constexpr int PULL_UNROLL = 8;         // halo slots whose DSMEM loads one thread keeps in flight
+constexpr int CHEB_KMAX = 4;           // cells per thread whose state stays in registers
 
 struct ChebArgs {
   const double* b;  // list-indexed rhs
