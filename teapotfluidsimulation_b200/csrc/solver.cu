@@ -550,7 +550,7 @@ int standalone_pcg(const uint8_t* cell, const double* b, double* q, int nx, int 
   char* p = static_cast<char*>(mem) + wsb;
   int* lidx = (int*)p;
   int* list = lidx + nc;
-  double* bl = (double*)(list + nc + (nc & 1));
+  double* bl = (double*)(list + nc);  // 2 * nc ints from a 256-byte boundary: 8-byte aligned
   double* ql = bl + nc;
   int* small = (int*)(ql + nc);  // [0] m, [1..2] result
   double* resd = (double*)(small + 4);

@@ -226,6 +226,26 @@ def test_standalone_pcg_matches_oracle(engine, oracle_mod):
     assert not conv
 
 
+def test_standalone_pcg_odd_sized_grid(engine, oracle_mod):
+    # an odd cell count (9 x 7 x 5) places the solver's FP64 scratch after an odd number of ints
+    import torch
+
+    nx, ny, nz = 9, 7, 5
+    rng = np.random.default_rng(3)
+    cell = np.full(nx * ny * nz, 2, np.uint8)
+    for k in range(1, nz - 1):
+        for j in range(1, ny - 1):
+            for i in range(1, nx - 1):
+                cell[i + nx * (j + ny * k)] = 1 if j < 4 else 0
+    b = np.where(cell == 1, rng.standard_normal(cell.size), 0.0)
+    q0, it0, conv0, _ = oracle_mod.pcg_solve(cell, b, nx, ny, nz, 1e-10, 200)
+    dc, db = torch.tensor(cell, device="cuda"), torch.tensor(b, device="cuda")
+    dq = torch.zeros(cell.size, dtype=torch.float64, device="cuda")
+    it, conv, _ = engine.pcg_solve_device(dc.data_ptr(), db.data_ptr(), dq.data_ptr(), nx, ny, nz, 1e-10, 200)
+    assert conv and conv0 and it == it0
+    assert rel_l2(dq.cpu().numpy(), q0) < 1e-12
+
+
 @pytest.mark.slow
 def test_whole_pour_5mm_against_reference(engine, goldens):
     # benchmarks/run3d.json 5 mm: 406.78 mL, shares 27.71 / 51.94 / 20.35 %, nothing spilled or lost
