@@ -799,4 +799,15 @@ int pl_pcg_solve_device(const uint8_t* cell, const double* b, double* q, int32_t
   return PL_OK;
 }
 
+int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny,
+                                int32_t nz, double tol, int32_t max_iter, void* stream, int32_t* iterations,
+                                int32_t* converged, double* residual) {
+  if (!cell || !b || !q) return fail(PL_E_ARG, "pl_pcg_solve_device_noalloc: null buffer");
+  char err[256] = "";
+  int rc = standalone_pcg_noalloc(cell, b, q, nx, ny, nz, tol, max_iter, (cudaStream_t)stream, iterations,
+                                  converged, residual, err, sizeof err);
+  if (rc) return fail(rc, "%s", err);
+  return PL_OK;
+}
+
 }  // extern "C"

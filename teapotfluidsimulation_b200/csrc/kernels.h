@@ -54,5 +54,9 @@ void launch_export_correction(const Geo& g, const DevPtrs& P, float* out, cudaSt
 int standalone_pcg(const uint8_t* cell, const double* b, double* q, int nx, int ny, int nz, double tol,
                    int max_iter, int precond, int precision, cudaStream_t st, int* iterations, int* converged,
                    double* residual, char* err, size_t errlen);
+// The same solve with fixed static scratch (pl_pcg_solve_device_noalloc); allocates nothing.
+int standalone_pcg_noalloc(const uint8_t* cell, const double* b, double* q, int nx, int ny, int nz, double tol,
+                           int max_iter, cudaStream_t st, int* iterations, int* converged, double* residual,
+                           char* err, size_t errlen);
 
 }  // namespace pl

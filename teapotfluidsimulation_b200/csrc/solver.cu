@@ -10,6 +10,7 @@
 // are fixed-order tree reductions (deterministic; they differ from the reference's sequential sums
 // only in rounding).
 #include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -566,6 +567,110 @@ int standalone_pcg(const uint8_t* cell, const double* b, double* q, int nx, int 
   cudaError_t ef = cudaFree(mem);
   if (e != cudaSuccess || ef != cudaSuccess) {
     snprintf(err, errlen, "pl_pcg_solve_device: %s", cudaGetErrorString(e != cudaSuccess ? e : ef));
+    return PL_E_CUDA;
+  }
+  if (iterations) *iterations = hres[1];
+  if (converged) *converged = hres[2];
+  if (residual) *residual = hr;
+  return PL_OK;
+}
+
+// ---------------------------------------------------------------- standalone solve, fixed scratch
+
+// The same solve with its scratch in this module's static device memory instead of cudaMalloc, for
+// hosts that own all device memory themselves (a pool or arena they hand out, a budget that forbids
+// allocations outside it) and so cannot let a library call cudaMalloc/cudaFree on their behalf.
+// The scratch covers grids of up to PL_NOALLOC_MAX_CELLS cells: the solver workspace, the cell-to-
+// list map, the liquid list, the list-ordered rhs and solution and the result slots (~30 MB).
+// Nothing in it has to start at zero: every word a kernel reads was written earlier in the same
+// call. One copy exists per device, so calls that overlap on one device (two host threads, or a
+// second call while the first is still running) overwrite each other's scratch.
+constexpr size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t NOALLOC_WS_BYTES = 8 * al256((size_t)PL_NOALLOC_MAX_CELLS * 8) +
+                                    al256((size_t)PL_NOALLOC_MAX_CELLS * 24) +
+                                    2 * al256((size_t)PL_NOALLOC_MAX_CELLS * 4) +
+                                    al256((MAX_LEVELS + 1) * 4) + al256(16);
+constexpr size_t NOALLOC_BYTES = NOALLOC_WS_BYTES + (size_t)PL_NOALLOC_MAX_CELLS * (4 * 2 + 8 * 2) + 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_base[NOALLOC_MAX_DEVICES];
+
+// Device address of the current device's scratch. The first call on a device looks it up with
+// cudaGetSymbolAddress while that device is current (the host-side name of the array is only a
+// handle for the lookup, never an address a kernel may use) and keeps it for later calls.
+static int noalloc_scratch(void** base, char* err, size_t errlen) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "pl_pcg_solve_device_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+    return PL_E_CUDA;
+  }
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+    snprintf(err, errlen, "pl_pcg_solve_device_noalloc: device %d beyond the %d supported", dev,
+             NOALLOC_MAX_DEVICES);
+    return PL_E_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      snprintf(err, errlen, "pl_pcg_solve_device_noalloc: cudaGetSymbolAddress on device %d: %s", dev,
+               e != cudaSuccess ? cudaGetErrorString(e) : "null address");
+      return PL_E_CUDA;
+    }
+    g_noalloc_base[dev] = p;
+  }
+  *base = g_noalloc_base[dev];
+  return PL_OK;
+}
+
+int standalone_pcg_noalloc(const uint8_t* cell, const double* b, double* q, int nx, int ny, int nz, double tol,
+                           int max_iter, cudaStream_t st, int* iterations, int* converged, double* residual,
+                           char* err, size_t errlen) {
+  if (nx < 3 || ny < 3 || nz < 3 || nx + ny + nz > MAX_LEVELS) {
+    snprintf(err, errlen, "pl_pcg_solve_device_noalloc: grid %dx%dx%d out of range", nx, ny, nz);
+    return PL_E_ARG;
+  }
+  const long long ncl = (long long)nx * ny * nz;
+  if (ncl > PL_NOALLOC_MAX_CELLS) {
+    snprintf(err, errlen,
+             "pl_pcg_solve_device_noalloc: grid %dx%dx%d has %lld cells, more than the fixed scratch holds "
+             "(PL_NOALLOC_MAX_CELLS = %d); use pl_pcg_solve_device",
+             nx, ny, nz, ncl, PL_NOALLOC_MAX_CELLS);
+    return PL_E_ARG;
+  }
+  const int nc = (int)ncl;
+  const size_t wsb = solver_ws_bytes(nc);
+  if (wsb + (size_t)nc * (4 * 2 + 8 * 2) + 256 > NOALLOC_BYTES) {  // cannot happen for nc <= the maximum
+    snprintf(err, errlen, "pl_pcg_solve_device_noalloc: scratch layout exceeds %zu bytes", NOALLOC_BYTES);
+    return PL_E_ARG;
+  }
+  void* mem = nullptr;
+  int rc = noalloc_scratch(&mem, err, errlen);
+  if (rc) return rc;
+  SolverWs W = solver_ws_carve(mem, nc);
+  char* p = static_cast<char*>(mem) + wsb;
+  int* lidx = (int*)p;
+  int* list = lidx + nc;
+  double* bl = (double*)(list + nc);  // 2 * nc ints from a 256-byte boundary: 8-byte aligned
+  double* ql = bl + nc;
+  int* small = (int*)(ql + nc);  // [0] m, [1..2] result
+  double* resd = (double*)(small + 4);
+  k_standalone_prep<<<1, 1024, 0, st>>>(cell, nx, ny, nz, lidx, list, small);
+  k_standalone_setup<<<DENSITY_BLOCKS, 256, 0, st>>>(cell, b, nx, ny, lidx, list, small, W, bl);
+  k_standalone_pcg<<<1, SOLVER_THREADS, 0, st>>>(W, small, bl, ql, tol, max_iter, small + 1, resd);
+  k_standalone_scatter<<<(nc + 255) / 256, 256, 0, st>>>(lidx, ql, q, nc);
+  int hres[3];
+  double hr = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hres, small, 12, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hr, resd, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "pl_pcg_solve_device_noalloc: %s", cudaGetErrorString(e));
     return PL_E_CUDA;
   }
   if (iterations) *iterations = hres[1];

@@ -27,7 +27,7 @@ EXPORTED = [
     "pl_controller", "pl_get_diagnostics", "pl_discharged_fractions", "pl_read_particles",
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
     "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
-    "pl_stage_times", "pl_plan", "pl_autotune_solver",
+    "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -81,6 +81,8 @@ def lib() -> C.CDLL:
     L.pl_get_field.argtypes = [P, C.c_int32, P, C.c_size_t]
     L.pl_pcg_solve_device.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                                       C.c_int32, P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp]
+    L.pl_pcg_solve_device_noalloc.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32, P,
+                                              C.POINTER(C.c_int32), C.POINTER(C.c_int32), dp]
     L.pl_plan.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Sizes), dp, dp, dp, u8p]
     L.pl_autotune_solver.argtypes = [C.POINTER(abi.Config), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_float)]
@@ -311,4 +313,21 @@ def pcg_solve_device(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny: int, nz
     _check(lib().pl_pcg_solve_device(C.c_void_p(cell_ptr), C.c_void_p(b_ptr), C.c_void_p(q_ptr), nx, ny, nz, tol,
                                      max_iter, preconditioner, precision, C.c_void_p(stream), C.byref(it),
                                      C.byref(conv), C.byref(res)))
+    return it.value, bool(conv.value), res.value
+
+
+NOALLOC_MAX_CELLS = 262144  # PL_NOALLOC_MAX_CELLS
+
+
+def pcg_solve_device_noalloc(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny: int, nz: int, tol: float,
+                             max_iter: int, stream: int = 0):
+    """pcg_solve_device (MIC(0), FP64) with the library's fixed static scratch: allocates no device memory.
+
+    Grids above NOALLOC_MAX_CELLS cells raise EngineError; calls on one device must not overlap."""
+    it = C.c_int32()
+    conv = C.c_int32()
+    res = C.c_double()
+    _check(lib().pl_pcg_solve_device_noalloc(C.c_void_p(cell_ptr), C.c_void_p(b_ptr), C.c_void_p(q_ptr), nx, ny, nz,
+                                             tol, max_iter, C.c_void_p(stream), C.byref(it), C.byref(conv),
+                                             C.byref(res)))
     return it.value, bool(conv.value), res.value

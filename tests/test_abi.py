@@ -106,3 +106,9 @@ def test_missing_library_fails_loudly(tmp_path):
         ROOT, str(tmp_path / "nope.so"))
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout
     assert "raised True" in out
+
+
+def test_noalloc_limit_matches_header(engine):
+    text = open(os.path.join(ROOT, "include", "pourlab.h")).read()
+    m = re.search(r"#define PL_NOALLOC_MAX_CELLS (\d+)", text)
+    assert m and int(m.group(1)) == engine.engine.NOALLOC_MAX_CELLS
