@@ -326,7 +326,7 @@ def run_ours(args):
         wall += time.perf_counter() - t0
     e2e_s = e2e_sim.diagnostics()["time"] - e0
     e2e_value = allsum(e2e_s, world) / allmax(wall, world)
-    scalars = 400  # bytes of the device scalar block (SimScalars) copied each way per pl_step
+    scalars = int(e2e_sim.sizes.step_copy_bytes)  # the device scalar block, copied each way per pl_step
 
     peaks, peak_kind = measured_peaks()
     pres_ms = stage_acc.get("pressure", 0.0) / max(steps_done, 1)

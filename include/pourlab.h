@@ -150,7 +150,7 @@ typedef struct pl_sizes {
   double pivot_world[2];
   double fill_height;
   int32_t band_counts[3]; /* parcels per origin layer (bottom, middle, top) */
-  int32_t reserved;
+  int32_t step_copy_bytes; /* bytes pl_step copies to the device and back (the device scalar block) */
 } pl_sizes;
 
 /* PourController internal state (src/sim/motion.ts:21-38): enough to resume a run exactly. */
@@ -321,10 +321,11 @@ int pl_get_field(pl_sim* sim, int32_t field, void* out, size_t count);
 /* ------------------------------------------------------------------ standalone pressure solve */
 
 /* Pcg3D.solve(cell, b, q, tol, maxIter) (solver3d.ts:858-937) as a standalone call on
- * caller-provided device buffers: cell u8[nx*ny*nz], b and q f64[nx*ny*nz]. Runs the chosen
- * preconditioner on stream (0 = legacy default stream) and writes iterations, converged and
- * the final max-norm residual to host memory after synchronising. Scratch memory is allocated
- * by the call and freed before it returns. */
+ * caller-provided device buffers: cell u8[nx*ny*nz], b and q f64[nx*ny*nz]. Runs the reference's
+ * MIC(0) preconditioner in FP64 (preconditioner must be PL_PRECOND_MIC0 and precision
+ * PL_SOLVE_F64; other values return PL_E_ARG) on stream (0 = legacy default stream) and writes
+ * iterations, converged and the final max-norm residual to host memory after synchronising.
+ * Scratch memory is allocated by the call and freed before it returns. */
 int pl_pcg_solve_device(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny,
                         int32_t nz, double tol, int32_t max_iter, int32_t preconditioner,
                         int32_t precision, void* stream, int32_t* iterations, int32_t* converged,

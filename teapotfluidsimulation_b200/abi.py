@@ -147,7 +147,7 @@ class Sizes(C.Structure):
         ("pivot_world", C.c_double * 2),
         ("fill_height", C.c_double),
         ("band_counts", C.c_int32 * 3),
-        ("reserved", C.c_int32),
+        ("step_copy_bytes", C.c_int32),
     ]
 
 

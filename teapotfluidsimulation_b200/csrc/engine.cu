@@ -371,6 +371,7 @@ int pl_plan(const pl_config* cfg, pl_sizes* o, double* x, double* y, double* z, 
   o->pivot_world[1] = g.pwy;
   o->fill_height = init.fill_height;
   for (int k = 0; k < 3; k++) o->band_counts[k] = init.band_counts[k];
+  o->step_copy_bytes = int32_t(sizeof(SimScalars));
   const size_t n = size_t(g.n);
   if (x) std::memcpy(x, init.x.data(), n * 8);
   if (y) std::memcpy(y, init.y.data(), n * 8);
@@ -482,6 +483,7 @@ int pl_get_sizes(const pl_sim* s, pl_sizes* o) {
   o->pivot_world[1] = s->g.pwy;
   o->fill_height = s->fill_height;
   for (int k = 0; k < 3; k++) o->band_counts[k] = s->band_counts[k];
+  o->step_copy_bytes = int32_t(sizeof(SimScalars));
   return PL_OK;
 }
 

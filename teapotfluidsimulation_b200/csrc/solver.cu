@@ -532,8 +532,11 @@ __global__ void k_standalone_scatter(const int* lidx, const double* ql, double* 
 int standalone_pcg(const uint8_t* cell, const double* b, double* q, int nx, int ny, int nz, double tol,
                    int max_iter, int precond, int precision, cudaStream_t st, int* iterations, int* converged,
                    double* residual, char* err, size_t errlen) {
-  (void)precond;
-  (void)precision;
+  if (precond != PL_PRECOND_MIC0 || precision != PL_SOLVE_F64) {
+    snprintf(err, errlen, "pl_pcg_solve_device: the standalone solve is MIC(0) in FP64 (preconditioner %d, "
+             "precision %d requested)", precond, precision);
+    return PL_E_ARG;
+  }
   if (nx < 3 || ny < 3 || nz < 3 || nx + ny + nz > MAX_LEVELS) {
     snprintf(err, errlen, "pl_pcg_solve_device: grid %dx%dx%d out of range", nx, ny, nz);
     return PL_E_ARG;
