@@ -1057,7 +1057,7 @@ int plo_get_sizes(const plo_sim* s, pl_sizes* o) {
   o->pivot_world[0] = s->pivotWorld[0], o->pivot_world[1] = s->pivotWorld[1];
   o->fill_height = s->fillHeight;
   for (int k = 0; k < 3; k++) o->band_counts[k] = s->bandCounts[k];
-  o->reserved = 0;
+  o->step_copy_bytes = 0;  // no device scalar block on the CPU
   return PL_OK;
 }
 
