@@ -116,7 +116,7 @@ typedef struct pl_config {
   int32_t solve_precision; /* enum pl_solve_precision */
   int32_t device;          /* CUDA device ordinal; -1 = the calling thread's current device */
   int32_t solve_cluster;   /* CTAs of the cluster solves (1-16; 0 = 16), see pl_autotune_solver */
-  int32_t solve_threads;   /* threads per CTA of the cluster solves (32-512; 0 = 256) */
+  int32_t solve_threads;   /* threads per CTA of the cluster solves (32-1024; 0 = 512) */
   int32_t reserved[3];
 } pl_config;
 

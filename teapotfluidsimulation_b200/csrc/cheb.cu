@@ -3,31 +3,43 @@
 // Preconditioner: z = p(D^-1 A) D^-1 r, `degree` Chebyshev steps for D^-1 A on [lo, 2] from z = 0
 // (the WebGPU port's preconditioner, src/gpu3d/shaders.ts:588-622). The polynomial is positive on
 // (0, 2], so the preconditioner is symmetric positive definite and CG stays valid; every step is one
-// 7-point stencil with no inner products. On these free-surface systems it needs about as many
-// stencil applications as the best geometric multigrid variants while using a single level, so a
-// CG iteration is `degree + 1` cluster phases and there is no hierarchy to build.
+// 7-point stencil with no inner products.
 //
-// Layout: the liquid list (index order) is split into `cluster` contiguous ranges, one per CTA, and
-// each thread owns up to CHEB_KMAX cells of its CTA's range. Everything a cell needs only for itself
-// (residuals, inverse diagonal, solution, neighbour indices) stays in the owning thread's registers;
-// the stencil vectors (Chebyshev direction, z, CG direction, and q in FP32 mode) live in shared
-// memory, own cells first, then a zero guard element, then one halo slot per reference to a cell of
-// another CTA. A CTA never reads another CTA's shared memory while solving: whenever a thread
-// computes a new value of a stencil vector it stores it locally and also writes it straight into the
-// halo slots that reference it in other CTAs (DSMEM stores, which need no round trip), and the
-// cluster barrier that ends the phase publishes both. The destinations of each cell are learnt once,
-// in the prologue, from the other CTAs' requests. Vectors are double-buffered where a phase writes
-// what the same phase reads.
+// Partition: the liquid cells in column-tile order (8 x 8 columns, then k, j, i; built by
+// k_solve_setup) are split into `cluster` contiguous ranges, one per CTA, so each CTA owns a compact
+// block and exchanges only its faces. Each thread owns up to CHEB_KMAX cells; their per-cell state
+// (residuals, diagonal, solution, neighbour indices) stays in registers. Stencil vectors live in
+// shared memory: own cells, a zero guard element, then one halo slot per remote cell that some own
+// cell references (deduplicated: a remote cell has one slot however many own neighbours it has).
 //
-// Reductions are deterministic: per-thread partials in cell order, warps in order, then each CTA's
-// partial is written into every CTA's slot table and each CTA sums the slots in rank order.
+// Exchange (one "round" per stencil vector): the thread that computes a new value of a boundary cell
+// stores it locally and writes it straight into the halo slot of every CTA that requested the cell
+// with st.async, which also completes those bytes on that CTA's exchange mbarrier. A CTA then waits
+// only for its own barrier (it expects one value per halo slot), so no round needs a cluster-wide
+// barrier, and the halo traffic is one value per (boundary cell, requesting CTA). Two buffers and
+// two barriers alternate by round parity: a CTA can run at most one round ahead of a neighbour,
+// because it needs that neighbour's values of the previous round, which the neighbour sends only
+// after it has read everything of the round before.
 //
-// Stopping rule and bookkeeping: the reference's (solver3d.ts:858-937), max-norm residual
-// <= max(tol * max|b|, 1e-14), breakdown if s.As <= 0; like the WebGPU port the preconditioner
-// runs before the convergence test so that max|r| and z.r share one reduction. With FP32 vectors
-// (PL_SOLVE_MIXED) a recursive-residual convergence is confirmed by the FP64 true residual
-// b - A q and CG restarts from it when it misses the target (iterative refinement).
+// Reductions are deterministic and also barrier-free: every CTA folds its warps' partials in warp
+// order, sends the result to every other CTA's slot table (st.async on their reduction barrier), and
+// sums the slots in rank order, its own partial in its own place.
+//
+// CG (Chronopoulos-Gear ordering): after z = M r each CTA forms w = A z from the exchanged z, and one
+// reduction gives max|r|, z.r and z.w; s = z + beta s and A s = w + beta A s follow without another
+// exchange, and s.As = z.w - beta z.r / alpha_prev. The stopping rule and bookkeeping are the
+// reference's (solver3d.ts:858-937): max-norm residual <= max(tol * max|b|, 1e-14), breakdown if
+// s.As <= 0, the same iteration count; like the WebGPU port the preconditioner runs before the
+// convergence test so that max|r| and z.r share one reduction. With FP32 vectors (PL_SOLVE_MIXED) a
+// recursive-residual convergence is confirmed by the FP64 true residual b - A q and CG restarts from
+// it when it misses the target (iterative refinement).
+//
+// Every wait is bounded (CHEB_WAIT_LIMIT polls): a wait that gives up sets ERR_SOLVER_TIMEOUT and
+// the solve still runs every round to the end, so no CTA is left waiting and none exits while
+// another can still write into its shared memory.
 #include <cooperative_groups.h>
+
+#include <algorithm>
 
 #include "cheb.h"
 
@@ -37,44 +49,158 @@ namespace pl {
 
 namespace {
 
+constexpr int CHEB_WAIT_LIMIT = 1 << 20;
+constexpr int CHEB_MAX_DEGREE = 32;
+constexpr int CHEB_BITMAP_WORDS = 1024;  // remote-reference bitmap over liquid positions (<= 32768)
+
+__device__ __forceinline__ uint32_t s_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Shared::cluster address of the same shared-memory location in CTA `rank`.
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
+  uint32_t o;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(o) : "r"(a), "r"(rank));
+  return o;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// This CTA's arrival on its barrier, announcing the bytes the current phase receives.
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase of the given parity to complete; clears ok when the poll limit runs out, and
+// once ok is clear no longer waits (so a failed solve runs its remaining rounds without stalling).
+__device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, bool& ok) {
+  if (!ok) return;
+  for (int i = 0; i < CHEB_WAIT_LIMIT; i++)
+    if (mbar_try(bar, parity)) return;
+  ok = false;
+}
+
+// Remote store that completes its bytes on the destination CTA's barrier.
+__device__ __forceinline__ void st_async(uint32_t raddr, float v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(raddr),
+               "r"(__float_as_uint(v)), "r"(rbar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t raddr, double v, uint32_t rbar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(raddr),
+               "l"(__double_as_longlong(v)), "r"(rbar)
+               : "memory");
+}
+
+// Shared-memory accesses by 32-bit address (volatile: they keep their order against the barrier waits).
+__device__ __forceinline__ double lds(uint32_t a, double) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float lds(uint32_t a, float) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts(uint32_t a, double v) {
+  asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void sts(uint32_t a, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
 struct Cl {
-  char* base[CHEB_CLUSTER];  // generic address of every rank's dynamic shared memory
-  double2 slot[2][CHEB_CLUSTER];
-  double2 wpart[CHEB_MAX_THREADS / 32];
-  int out_cnt[CHEB_CLUSTER];  // requests this rank sends to each owner
+  unsigned long long xbar[2];    // exchange barriers (round parity)
+  unsigned long long rbar[2];    // reduction barriers (reduction parity)
+  uint32_t rsmem[CHEB_CLUSTER];  // shared::cluster address of every rank's dynamic shared memory
+  uint32_t rxbar[CHEB_CLUSTER];  // ... of every rank's xbar[0]
+  uint32_t rrbar[CHEB_CLUSTER];  // ... of every rank's rbar[0]
+  uint32_t rred[CHEB_CLUSTER];   // ... of every rank's red[0][0][0]
+  double red[2][CHEB_CLUSTER][3];  // reduction slots: (max, sum, sum) from each rank
+  double wpart[2][CHEB_MAX_THREADS / 32][3];
+  double bcast[2][3];
+  double coef[CHEB_MAX_DEGREE][2];  // Chebyshev step coefficients (c1, c2)
+  int out_cnt[CHEB_CLUSTER];  // distinct remote cells this rank references in each owner
   int in_cnt[CHEB_CLUSTER];   // requests each rank sends to this rank
   int out_pos[CHEB_CLUSTER];  // running position of this rank's requests in each owner's table
-  int nh;
-  int hcap;
+  int nh;                     // halo slots of this rank
 };
 
-// Deterministic cluster-wide (max of x, sum of y) in one barrier.
-__device__ double2 reduce2(double mx, double sm, Cl& C, int& phase, int me, int ns, cg::cluster_group& cl) {
+// Deterministic cluster-wide (max x, sum y, sum z). Xor butterflies leave the same bits in every
+// lane (their additions pair the same operands in every lane), so: each warp reduces its lanes;
+// warp 0 reduces the warp partials (lane w holds warp w's) into the CTA partial, sends it to every
+// other rank's slot table (st.async on their reduction barrier), waits for theirs, and reduces the
+// rank partials (lane q holds rank q's, its own in its own place) in the same fixed tree, so every
+// rank gets the same bits; the result is broadcast through shared memory.
+__device__ __forceinline__ void butterfly3(double& mx, double& s1, double& s2) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mx = dmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    sm += __shfl_xor_sync(0xffffffffu, sm, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
   }
-  if ((threadIdx.x & 31) == 0) C.wpart[threadIdx.x >> 5] = make_double2(mx, sm);
+}
+
+__device__ double3 reduce3(double mx, double s1, double s2, Cl& C, int& rr, int me, int ns, bool& ok) {
+  butterfly3(mx, s1, s2);
+  const int sl = rr & 1;
+  const uint32_t par = uint32_t(rr >> 1) & 1u;
+  rr++;
+  const int lane = int(threadIdx.x & 31), wid = int(threadIdx.x >> 5);
+  if (lane == 0) {
+    C.wpart[sl][wid][0] = mx;
+    C.wpart[sl][wid][1] = s1;
+    C.wpart[sl][wid][2] = s2;
+  }
   __syncthreads();
-  const int sl = phase & 1;
-  phase++;
-  if (threadIdx.x < ns) {
-    double2 t = make_double2(0.0, 0.0);
-    for (int w = 0; w < int(blockDim.x >> 5); w++) {
-      t.x = dmax(t.x, C.wpart[w].x);
-      t.y += C.wpart[w].y;
+  if (wid == 0) {
+    const int nw = int(blockDim.x >> 5);
+    double a = 0, b = 0, c = 0;  // all maxima reduced here are of non-negative values
+    if (lane < nw) {
+      a = C.wpart[sl][lane][0];
+      b = C.wpart[sl][lane][1];
+      c = C.wpart[sl][lane][2];
     }
-    Cl* dst = cl.map_shared_rank(&C, int(threadIdx.x));
-    dst->slot[sl][me] = t;
+    butterfly3(a, b, c);
+    if (lane == 0) mbar_expect(s_addr(&C.rbar[sl]), uint32_t(ns - 1) * 24u);
+    if (lane < ns && lane != me) {
+      const uint32_t dst = C.rred[lane] + uint32_t((sl * CHEB_CLUSTER + me) * 24);
+      const uint32_t bar = C.rrbar[lane] + uint32_t(sl * 8);
+      st_async(dst, a, bar);
+      st_async(dst + 8, b, bar);
+      st_async(dst + 16, c, bar);
+    }
+    mbar_wait(s_addr(&C.rbar[sl]), par, ok);
+    double x = 0, y = 0, z = 0;
+    if (lane == me) {
+      x = a;
+      y = b;
+      z = c;
+    } else if (lane < ns) {
+      x = C.red[sl][lane][0];
+      y = C.red[sl][lane][1];
+      z = C.red[sl][lane][2];
+    }
+    butterfly3(x, y, z);
+    if (lane == 0) {
+      C.bcast[sl][0] = x;
+      C.bcast[sl][1] = y;
+      C.bcast[sl][2] = z;
+    }
   }
-  cl.sync();
-  double2 t = make_double2(0.0, 0.0);
-  for (int r = 0; r < ns; r++) {
-    t.x = dmax(t.x, C.slot[sl][r].x);
-    t.y += C.slot[sl][r].y;
-  }
-  return t;
+  __syncthreads();
+  return make_double3(C.bcast[sl][0], C.bcast[sl][1], C.bcast[sl][2]);
 }
 
 // Element i of the shared-memory array at byte offset `off`.
@@ -85,11 +211,13 @@ __device__ __forceinline__ V& sv(char* smem, uint32_t off, int i) {
 
 }  // namespace
 
-template <typename T>
-__global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, SolverWs W, ChebArgs a) {
-  constexpr int K = CHEB_KMAX;
+// K: cells per thread (1, 2 or 4; at most 1024 / K threads, so that the per-cell state stays in
+// registers).
+template <typename T, int K>
+__global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs P, SolverWs W, ChebArgs a) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
+  if (a.gate && sc->mg_status) return;  // the launch before this one solved the system
   if (a.is_correction) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // interior mean of the density ratios (solver3d.ts:670)
       double s = 0;
@@ -113,6 +241,7 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, 
   const int ns = int(cl.num_blocks());
   const int me = int(cl.block_rank());
   const int nt = int(blockDim.x);
+  const int tid = int(threadIdx.x);
   extern __shared__ __align__(16) char smem[];
   __shared__ Cl C;
   __shared__ int s_warp[CHEB_MAX_THREADS / 32];
@@ -121,65 +250,113 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, 
   const int own0 = me * chunk;
   const int cnt = m > own0 ? min(own0 + chunk, m) - own0 : 0;
   const int guard = chunk;  // element [chunk] of every stencil vector is 0; halo slots follow it
-  if ((chunk + nt - 1) / nt > K) {  // uniform: more cells per thread than registers hold
-    if (me == 0 && threadIdx.x == 0) sc->mg_status = 0;
+  const int deg = a.degree;
+  // uniform decisions: more cells per thread than registers hold, or a polynomial degree or a
+  // liquid-cell count beyond the fixed tables: the wavefront solver takes over
+  if ((chunk + nt - 1) / nt > K || deg < 1 || deg > CHEB_MAX_DEGREE || m > CHEB_BITMAP_WORDS * 32) {
+    if (me == 0 && tid == 0) sc->mg_status = 0;
     return;
   }
-  if (threadIdx.x < ns) {
-    C.base[threadIdx.x] = (char*)cl.map_shared_rank((void*)smem, int(threadIdx.x));
-    C.out_cnt[threadIdx.x] = 0;
-    C.out_pos[threadIdx.x] = 0;
+  // bitmap of the referenced remote positions and its word prefix: a fixed place at the end of the
+  // dynamic shared memory (the layout below stays clear of it)
+  const uint32_t BM = uint32_t(a.smem_bytes) - CHEB_BITMAP_WORDS * 8;
+  const uint32_t BMP = BM + CHEB_BITMAP_WORDS * 4;
+  const int nwords = (m + 31) >> 5;
+  if (tid == 0) {
+    mbar_init(s_addr(&C.xbar[0]), 1);
+    mbar_init(s_addr(&C.xbar[1]), 1);
+    mbar_init(s_addr(&C.rbar[0]), 1);
+    mbar_init(s_addr(&C.rbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // Chebyshev recurrence coefficients on [lo, 2]
+    const double lo = a.cheb_lo, hi = 2.0;
+    const double theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma1 = theta / delta;
+    double rho = 1 / sigma1;
+    for (int s = 1; s < deg; s++) {
+      const double rhoN = 1 / (2 * sigma1 - rho);
+      C.coef[s][0] = rhoN * rho;
+      C.coef[s][1] = 2 * rhoN / delta;
+      rho = rhoN;
+    }
   }
+  if (tid < ns) {
+    C.rsmem[tid] = mapa_u32(s_addr(smem), tid);
+    C.rxbar[tid] = mapa_u32(s_addr(&C.xbar[0]), tid);
+    C.rrbar[tid] = mapa_u32(s_addr(&C.rbar[0]), tid);
+    C.rred[tid] = mapa_u32(s_addr(&C.red[0][0][0]), tid);
+    C.out_cnt[tid] = 0;
+    C.out_pos[tid] = 0;
+  }
+  for (int w = tid; w < nwords; w += nt) sv<uint32_t>(smem, BM, w) = 0u;
   __syncthreads();
-  int phase = 0;  // reduction slot parity (advances identically in every thread)
-  // ---- own cells: t_k = threadIdx.x + k * nt
-  int gnb[K][6];  // neighbour list indices (prologue only)
-  int myrem = 0;
+  // ---- own cells t_k = tid + k * nt at tile-order positions own0 + t_k
+  int gnb[K][6];
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    const int t = threadIdx.x + k * nt;
+    const int t = tid + k * nt;
 #pragma unroll
-    for (int e = 0; e < 6; e++) {
-      int gi = t < cnt ? W.nb[e * W.cap + own0 + t] : -1;
-      gnb[k][e] = gi;
-      if (gi >= 0 && gi / chunk != me) {
-        myrem++;
-        atomicAdd(&C.out_cnt[gi / chunk], 1);
+    for (int f = 0; f < 6; f++) {
+      const int gi = t < cnt ? P.tnb[f * g.nc + own0 + t] : -1;
+      gnb[k][f] = gi;
+      if (gi >= 0 && gi / chunk != me) atomicOr(&sv<uint32_t>(smem, BM, gi >> 5), 1u << (gi & 31));
+    }
+  }
+  __syncthreads();
+  // halo slot of a remote position = its rank among the referenced positions (so the slots of one
+  // owner are contiguous and ordered by position)
+  {
+    const int per = (nwords + nt - 1) / nt;
+    const int w0 = tid * per;
+    int sum = 0;
+    for (int q = 0; q < per; q++)
+      if (w0 + q < nwords) sum += __popc(sv<uint32_t>(smem, BM, w0 + q));
+    const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (tid == 0) {
+      int acc = 0;
+      for (int w = 0; w < nw; w++) {
+        int c = s_warp[w];
+        s_warp[w] = acc;
+        acc += c;
       }
+      C.nh = acc;
     }
+    __syncthreads();
+    int run = s_warp[wid] + x - sum;
+    for (int q = 0; q < per; q++)
+      if (w0 + q < nwords) {
+        sv<int>(smem, BMP, w0 + q) = run;
+        run += __popc(sv<uint32_t>(smem, BM, w0 + q));
+      }
   }
-  // halo slots: block-exclusive scan of the per-thread remote counts
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = nt >> 5;
-  int x = myrem;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[wid] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int w = 0; w < nw; w++) {
-      int c = s_warp[w];
-      s_warp[w] = acc;
-      acc += c;
-    }
-    C.nh = acc;
-  }
+  auto hrank = [&](int gi) {  // referenced remote positions before gi
+    if (gi >= m) return C.nh;
+    const int w = gi >> 5;
+    return sv<int>(smem, BMP, w) + __popc(sv<uint32_t>(smem, BM, w) & ((1u << (gi & 31)) - 1u));
+  };
+  if (tid < ns && tid != me) C.out_cnt[tid] = hrank(min((tid + 1) * chunk, m)) - hrank(min(tid * chunk, m));
+  __syncthreads();
   // tell every owner how many requests it gets from this rank
-  if (threadIdx.x < ns) {
-    Cl* dst = cl.map_shared_rank(&C, int(threadIdx.x));
-    dst->in_cnt[me] = C.out_cnt[threadIdx.x];
+  if (tid < ns) {
+    Cl* dst = cl.map_shared_rank(&C, tid);
+    dst->in_cnt[me] = C.out_cnt[tid];
   }
-  __syncthreads();
-  int hslot = s_warp[wid] + x - myrem;
+  cl.sync();  // in_cnt complete everywhere; barrier initialisation visible to the cluster
+  const int nh = C.nh;
   int incoming = 0;
-  cl.sync();  // in_cnt complete everywhere
   for (int r = 0; r < ns; r++) incoming += C.in_cnt[r];
-  const double2 caps = reduce2(double(C.nh), double(0), C, phase, me, ns, cl);
-  const int hcap = int(caps.x);
-  int inmax = int(reduce2(double(incoming), 0.0, C, phase, me, ns, cl).x);
+  int rr = 0;  // reduction counter (advances identically in every thread)
+  int e = 0;   // exchange-round counter (likewise)
+  bool ok = true;
+  const int hcap = int(reduce3(double(nh), 0.0, 0.0, C, rr, me, ns, ok).x);
   // ---- layout (identical in every rank): byte offsets into the dynamic shared memory
   uint32_t off = 0;
   auto take = [&](size_t bytes) -> uint32_t {
@@ -188,228 +365,260 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, 
     return r;
   };
   const int n1 = chunk + 1 + hcap;  // own cells, guard, halo
-  const uint32_t CD0 = take(size_t(n1) * sizeof(T)), CD1 = take(size_t(n1) * sizeof(T));
+  const uint32_t DV0 = take(size_t(n1) * sizeof(T)), DV1 = take(size_t(n1) * sizeof(T));
   const uint32_t ZS = take(size_t(n1) * sizeof(T));
-  const uint32_t S0 = take(size_t(n1) * sizeof(T)), S1 = take(size_t(n1) * sizeof(T));
   const uint32_t QS = take(size_t(n1) * 8);
   const uint32_t DCNT = take(size_t(chunk) * 4);
-  const uint32_t DST = take(size_t(chunk) * 24);       // up to 6 destinations per own cell
-  const uint32_t REQ = take(size_t(inmax) * 8 + 8);  // (own local index, rank << 16 | slot)
-  if (off > uint32_t(a.smem_bytes) || n1 > 65535) {  // uniform decision: the wavefront solver takes over
-    if (me == 0 && threadIdx.x == 0) sc->mg_status = 0;
+  const uint32_t DST = take(size_t(chunk) * 6 * 4);  // up to 6 requesting ranks per own cell
+  const uint32_t REQ = take(size_t(chunk) * 6 * 8);  // (own local index, rank << 16 | slot)
+  if (off > BM || n1 > 65535) {  // uniform decision: the wavefront solver takes over
+    if (me == 0 && tid == 0) sc->mg_status = 0;
     cl.sync();
     return;
   }
   // my requests' offset in each owner's table: the requests of lower ranks come first
-  if (threadIdx.x < ns) {
-    const Cl* own = cl.map_shared_rank(&C, int(threadIdx.x));
+  if (tid < ns) {
+    const Cl* own = cl.map_shared_rank(&C, tid);
     int o = 0;
     for (int r = 0; r < me; r++) o += own->in_cnt[r];
-    C.out_pos[threadIdx.x] = o;
+    C.out_pos[tid] = o;
   }
-  for (int i = threadIdx.x; i < n1; i += nt) {
-    sv<T>(smem, CD0, i) = sv<T>(smem, CD1, i) = sv<T>(smem, ZS, i) = T(0);
-    sv<T>(smem, S0, i) = sv<T>(smem, S1, i) = T(0);
+  for (int i = tid; i < n1; i += nt) {
+    sv<T>(smem, DV0, i) = sv<T>(smem, DV1, i) = sv<T>(smem, ZS, i) = T(0);
     sv<double>(smem, QS, i) = 0;
   }
-  for (int i = threadIdx.x; i < chunk; i += nt) sv<int>(smem, DCNT, i) = 0;
+  for (int i = tid; i < chunk; i += nt) sv<int>(smem, DCNT, i) = 0;
   __syncthreads();
-  // ---- requests: for each reference to another rank's cell, a halo slot here and an entry there
-  uint32_t nbl[K][3];  // local indices, two 16-bit halves per word
+  // ---- one request per referenced remote position, into its owner's table
+  for (int w = tid; w < nwords; w += nt) {
+    uint32_t bits = sv<uint32_t>(smem, BM, w);
+    int h = sv<int>(smem, BMP, w);
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1u;
+      const int gi = (w << 5) + b;
+      const int rk = gi / chunk;
+      const int pos = atomicAdd(&C.out_pos[rk], 1);
+      char* owner = static_cast<char*>(cl.map_shared_rank(static_cast<void*>(smem), rk));
+      reinterpret_cast<uint2*>(owner + REQ)[pos] =
+          make_uint2(uint32_t(gi - rk * chunk), (uint32_t(me) << 16) | uint32_t(h));
+      h++;
+    }
+  }
+  // byte offsets of the own cells' neighbours in a stencil vector of T (the guard for none)
+  uint32_t nbo[K][6];
+  bool has[K];
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    int li[6];
+    has[k] = tid + k * nt < cnt;
 #pragma unroll
-    for (int e = 0; e < 6; e++) {
-      const int gi = gnb[k][e];
-      if (gi < 0) {
-        li[e] = guard;
-      } else {
-        const int rk = gi / chunk;
-        if (rk == me) {
-          li[e] = gi - own0;
-        } else {
-          const int h = hslot++;
-          li[e] = guard + 1 + h;
-          const int pos = atomicAdd(&C.out_pos[rk], 1);
-          char* owner = C.base[rk];
-          reinterpret_cast<uint2*>(owner + REQ)[pos] = make_uint2(uint32_t(gi - rk * chunk), (uint32_t(me) << 16) | uint32_t(h));
-        }
-      }
+    for (int f = 0; f < 6; f++) {
+      const int gi = gnb[k][f];
+      const int li = gi < 0 ? guard : (gi / chunk == me ? gi - own0 : guard + 1 + hrank(gi));
+      nbo[k][f] = uint32_t(li) * uint32_t(sizeof(T));
     }
-    nbl[k][0] = uint32_t(li[0]) | (uint32_t(li[1]) << 16);
-    nbl[k][1] = uint32_t(li[2]) | (uint32_t(li[3]) << 16);
-    nbl[k][2] = uint32_t(li[4]) | (uint32_t(li[5]) << 16);
   }
-  cl.sync();  // every request is in its owner's table
-  for (int i = threadIdx.x; i < incoming; i += nt) {
+  cl.sync();  // every request is in its owner's table; no generic remote access after this
+  for (int i = tid; i < incoming; i += nt) {
     const uint2 rq = sv<uint2>(smem, REQ, i);
     const int p = atomicAdd(&sv<int>(smem, DCNT, int(rq.x)), 1);
     sv<uint32_t>(smem, DST, p * chunk + int(rq.x)) = rq.y;
   }
   __syncthreads();
   // ---- per-thread state of the owned cells
-  T r[K], z[K], res[K], as[K], sown[K], cdown[K], idg[K], dg[K];
+  T r[K], z[K], res[K], as[K], sown[K], cdown[K], idg[K], dg[K], w[K];
   double q[K], b64[K];
-  int ndst[K];
+  int nd[K];             // requesting ranks
+  uint32_t d0a[K], d0b[K];  // the first one's halo slot (in its vector at offset 0) and exchange barrier
   double bmax = 0;
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    const int t = threadIdx.x + k * nt;
-    const bool ok = t < cnt;
-    const double d = ok ? W.adiag[own0 + t] : 1.0;
+    const int t = tid + k * nt;
+    const int li = has[k] ? P.tperm[own0 + t] : 0;
+    const double d = has[k] ? W.adiag[li] : 1.0;
     dg[k] = T(d);
     idg[k] = T(1) / T(d);
-    b64[k] = ok ? a.b[own0 + t] : 0.0;
+    b64[k] = has[k] ? a.b[li] : 0.0;
     r[k] = T(b64[k]);
     q[k] = 0;
-    z[k] = res[k] = as[k] = sown[k] = cdown[k] = T(0);
-    ndst[k] = ok ? sv<int>(smem, DCNT, t) : 0;
+    z[k] = res[k] = as[k] = sown[k] = cdown[k] = w[k] = T(0);
+    nd[k] = has[k] ? sv<int>(smem, DCNT, t) : 0;
+    d0a[k] = d0b[k] = 0;
+    if (nd[k] > 0) {
+      const uint32_t dd = sv<uint32_t>(smem, DST, t);
+      const int rk = int(dd >> 16);
+      d0a[k] = C.rsmem[rk] + uint32_t(guard + 1 + int(dd & 0xffffu)) * uint32_t(sizeof(T));
+      d0b[k] = C.rxbar[rk];
+    }
     bmax = dmax(bmax, fabs(b64[k]));
   }
-  // Store v as own cell t_k of the vector at `voff` and into the halo slots that reference it.
-  auto put = [&](uint32_t voff, int k, auto v) {
-    using V = decltype(v);
-    const int t = threadIdx.x + k * nt;
-    sv<V>(smem, voff, t) = v;
-    for (int j = 0; j < ndst[k]; j++) {
-      const uint32_t d = sv<uint32_t>(smem, DST, j * chunk + t);
-      reinterpret_cast<V*>(C.base[d >> 16] + voff)[guard + 1 + int(d & 0xffffu)] = v;
+  const uint32_t sbase = s_addr(smem);
+  const uint32_t xb0 = s_addr(&C.xbar[0]);
+  // Store v (a T) as own cell t_k of the vector at byte offset voff and into the halo slots of the
+  // requesting ranks, on this round's barrier.
+  auto put = [&](uint32_t voff, int k, T v) {
+    const int t = tid + k * nt;
+    sts(sbase + voff + uint32_t(t) * uint32_t(sizeof(T)), v);
+    if (nd[k] > 0) {
+      const uint32_t bo = uint32_t(e & 1) * 8u;
+      st_async(d0a[k] + voff, v, d0b[k] + bo);
+      for (int j = 1; j < nd[k]; j++) {
+        const uint32_t dd = sv<uint32_t>(smem, DST, j * chunk + t);
+        const int rk = int(dd >> 16);
+        st_async(C.rsmem[rk] + voff + uint32_t(guard + 1 + int(dd & 0xffffu)) * uint32_t(sizeof(T)), v,
+                 C.rxbar[rk] + bo);
+      }
     }
   };
-  auto nsum = [&](uint32_t voff, int k) -> T {
-    const uint32_t w0 = nbl[k][0], w1 = nbl[k][1], w2 = nbl[k][2];
-    return sv<T>(smem, voff, w0 & 0xffff) + sv<T>(smem, voff, w0 >> 16) + sv<T>(smem, voff, w1 & 0xffff) +
-           sv<T>(smem, voff, w1 >> 16) + sv<T>(smem, voff, w2 & 0xffff) + sv<T>(smem, voff, w2 >> 16);
+  // The same for an FP64 vector (the solution q in the FP32 refinement).
+  auto put64 = [&](uint32_t voff, int k, double v) {
+    const int t = tid + k * nt;
+    sts(sbase + voff + uint32_t(t) * 8u, v);
+    const uint32_t bo = uint32_t(e & 1) * 8u;
+    for (int j = 0; j < nd[k]; j++) {
+      const uint32_t dd = sv<uint32_t>(smem, DST, j * chunk + t);
+      const int rk = int(dd >> 16);
+      st_async(C.rsmem[rk] + voff + uint32_t(guard + 1 + int(dd & 0xffffu)) * 8u, v, C.rxbar[rk] + bo);
+    }
   };
-  const double bnorm = reduce2(bmax, 0.0, C, phase, me, ns, cl).x;
-  const double lo = a.cheb_lo, hi = 2.0;
-  const double theta = (hi + lo) / 2, delta = (hi - lo) / 2;
-  const double sigma1 = theta / delta;
-  const int deg = a.degree;
+  // End of an exchange round of values of vbytes bytes: own values visible to the CTA, every halo
+  // slot received.
+  auto round_end = [&](uint32_t vbytes) {
+    const uint32_t bar = xb0 + uint32_t(e & 1) * 8u;
+    if (tid == 0) mbar_expect(bar, uint32_t(nh) * vbytes);
+    __syncthreads();
+    mbar_wait(bar, uint32_t(e >> 1) & 1u, ok);
+    e++;
+  };
+  // Sum of the six neighbour values of own cell k in the vector at byte offset voff (pairwise: three
+  // dependent additions).
+  auto nsum = [&](uint32_t voff, int k) -> T {
+    const uint32_t vb = sbase + voff;
+    const T x0 = lds(vb + nbo[k][0], T()), x1 = lds(vb + nbo[k][1], T()), x2 = lds(vb + nbo[k][2], T());
+    const T x3 = lds(vb + nbo[k][3], T()), x4 = lds(vb + nbo[k][4], T()), x5 = lds(vb + nbo[k][5], T());
+    return ((x0 + x1) + (x2 + x3)) + (x4 + x5);
+  };
+  const double bnorm = reduce3(bmax, 0.0, 0.0, C, rr, me, ns, ok).x;
+  const T itheta = T(2.0 / (2.0 + a.cheb_lo));
+  // z = p(D^-1 A) D^-1 r, published (own cells and halo) in ZS
+  auto precondition = [&]() {
+    uint32_t out = deg > 1 ? ((e & 1) ? DV1 : DV0) : ZS;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!has[k]) continue;
+      const T d = r[k] * idg[k] * itheta;
+      cdown[k] = d;
+      z[k] = d;
+      res[k] = r[k];
+      put(out, k, d);
+    }
+    uint32_t last = out;
+    round_end(sizeof(T));
+    for (int s = 1; s < deg; s++) {
+      const T c1 = T(C.coef[s][0]), c2 = T(C.coef[s][1]);
+      T acc[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) acc[k] = has[k] ? nsum(last, k) : T(0);
+      const bool final_step = s + 1 == deg;
+      out = final_step ? ZS : ((e & 1) ? DV1 : DV0);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        if (!has[k]) continue;
+        const T rs = res[k] - (dg[k] * cdown[k] - acc[k]);
+        res[k] = rs;
+        const T d = c1 * cdown[k] + c2 * rs * idg[k];
+        cdown[k] = d;
+        z[k] += d;
+        put(out, k, final_step ? z[k] : d);
+      }
+      last = out;
+      round_end(sizeof(T));
+    }
+  };
+  // w = A z from the published z; partial z.r and z.w
+  auto apply_z = [&](double* zr, double* zw) {
+    double pr = 0, pw = 0;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!has[k]) continue;
+      w[k] = dg[k] * z[k] - nsum(ZS, k);
+      pr += double(z[k]) * double(r[k]);
+      pw += double(z[k]) * double(w[k]);
+    }
+    *zr = pr;
+    *zw = pw;
+  };
   int iters = 0, converged = 1;
   double res_norm = bnorm;
   if (m > 0 && !(bnorm < 1e-14)) {
     const double target = dmax(a.tol * bnorm, 1e-14);
     converged = 0;
-    int cur = 0;  // CG direction buffer holding the current s
-    double sigma = 0, beta = 0;
     int restarts = 0;
-    bool fresh = true;  // s restarts from z
-    const T itheta = T(1.0 / theta);
-    // z = p(D^-1 A) D^-1 r; ends with z in ZS (own and halo), returns partial z.r and max|r|
-    auto precondition = [&](double* zr_out, double* rmax_out) {
-      int cdb = 0;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        if (threadIdx.x + k * nt >= cnt) continue;
-        const T d = r[k] * idg[k] * itheta;
-        cdown[k] = d;
-        z[k] = d;
-        res[k] = r[k];
-        if (deg > 1) put(CD0, k, d);
-      }
-      double rho = 1 / sigma1;
-      for (int s = 1; s < deg; s++) {
-        cl.sync();  // the previous direction is published (own cells and halos)
-        const uint32_t CO = cdb ? CD1 : CD0, CN = cdb ? CD0 : CD1;
-        const double rhoN = 1 / (2 * sigma1 - rho);
-        const T c1 = T(rhoN * rho), c2 = T(2 * rhoN / delta);
-        T acc[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) acc[k] = (threadIdx.x + k * nt < cnt) ? nsum(CO, k) : T(0);
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          if (threadIdx.x + k * nt >= cnt) continue;
-          const T rs = res[k] - (dg[k] * cdown[k] - acc[k]);
-          res[k] = rs;
-          const T d = c1 * cdown[k] + c2 * rs * idg[k];
-          cdown[k] = d;
-          z[k] += d;
-          if (s + 1 < deg) put(CN, k, d);
-        }
-        cdb ^= 1;
-        rho = rhoN;
-      }
-      double zr = 0, rm = 0;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        if (threadIdx.x + k * nt >= cnt) continue;
-        put(ZS, k, z[k]);
-        zr += double(z[k]) * double(r[k]);
-        rm = dmax(rm, fabs(double(r[k])));
-      }
-      *zr_out = zr;
-      *rmax_out = rm;
-    };
-    int it = 1;
+    bool fresh = true;
+    double gamma, delta, gamma_prev = 1, alpha_prev = 1;
     {
-      double zr, rm;
-      precondition(&zr, &rm);
-      sigma = reduce2(0.0, zr, C, phase, me, ns, cl).y;  // its barrier publishes z
+      double zr, zw;
+      precondition();
+      apply_z(&zr, &zw);
+      const double3 g3 = reduce3(0.0, zr, zw, C, rr, me, ns, ok);
+      gamma = g3.y;
+      delta = g3.z;
     }
+    int it = 1;
     for (; it <= a.max_iter; it++) {
-      // s = z + beta s and As = A s, the neighbours' s formed from their published z and old s
-      const T tb = T(fresh ? 0.0 : beta);
-      const uint32_t SO = cur ? S1 : S0, SN = cur ? S0 : S1;
-      double sp = 0;
-      T az[K], aso[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        const bool ok = threadIdx.x + k * nt < cnt;
-        az[k] = ok ? nsum(ZS, k) : T(0);
-        aso[k] = ok ? nsum(SO, k) : T(0);
+      double beta = 0, sas = delta;
+      if (!fresh) {
+        beta = gamma / gamma_prev;
+        sas = delta - beta * gamma / alpha_prev;
       }
+      if (!(sas > 0)) break;  // breakdown (solver3d.ts:913)
+      const double alpha = gamma / sas;
+      const T tb = T(beta), ta = T(alpha);
+      double rm = 0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        if (threadIdx.x + k * nt >= cnt) continue;
-        const T st = z[k] + tb * sown[k];
-        const T av = dg[k] * st - (az[k] + tb * aso[k]);
-        sown[k] = st;
-        as[k] = av;
-        put(SN, k, st);
-        sp += double(st) * double(av);
-      }
-      cur ^= 1;
-      fresh = false;
-      const double sas = reduce2(0.0, sp, C, phase, me, ns, cl).y;
-      if (!(sas > 0)) break;
-      const double alpha = sigma / sas;
-      const T ta = T(alpha);
-#pragma unroll
-      for (int k = 0; k < K; k++) {
+        if (!has[k]) continue;
+        sown[k] = z[k] + tb * sown[k];
+        as[k] = w[k] + tb * as[k];
         q[k] += alpha * double(sown[k]);
         r[k] = r[k] - ta * as[k];
+        rm = dmax(rm, fabs(double(r[k])));
       }
-      double zr, rm;
-      precondition(&zr, &rm);
-      const double2 both = reduce2(rm, zr, C, phase, me, ns, cl);  // max|r| and z.r in one barrier
-      res_norm = both.x;
+      double zr, zw;
+      precondition();
+      apply_z(&zr, &zw);
+      const double3 g3 = reduce3(rm, zr, zw, C, rr, me, ns, ok);  // max|r|, z.r, z.w in one round
+      res_norm = g3.x;
       if (res_norm <= target) {
-        if (sizeof(T) == 8 || restarts >= 4) {
+        if constexpr (sizeof(T) == 8) {
+          converged = 1;
+          break;
+        }
+        if (restarts >= 4) {
           converged = 1;
           break;
         }
         // FP32 vectors: confirm with the FP64 true residual b - A q
 #pragma unroll
         for (int k = 0; k < K; k++)
-          if (threadIdx.x + k * nt < cnt) put(QS, k, q[k]);
-        cl.sync();
+          if (has[k]) put64(QS, k, q[k]);
+        round_end(8);
         double tm = 0;
         T rt[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
           rt[k] = T(0);
-          if (threadIdx.x + k * nt >= cnt) continue;
-          const uint32_t w0 = nbl[k][0], w1 = nbl[k][1], w2 = nbl[k][2];
-          const double acc = sv<double>(smem, QS, w0 & 0xffff) + sv<double>(smem, QS, w0 >> 16) +
-                             sv<double>(smem, QS, w1 & 0xffff) + sv<double>(smem, QS, w1 >> 16) +
-                             sv<double>(smem, QS, w2 & 0xffff) + sv<double>(smem, QS, w2 >> 16);
+          if (!has[k]) continue;
+          const uint32_t qb = sbase + QS;
+          constexpr uint32_t sc8 = 8 / sizeof(T);  // FP64 offsets from the T offsets
+          const double acc = ((lds(qb + nbo[k][0] * sc8, 0.0) + lds(qb + nbo[k][1] * sc8, 0.0)) +
+                              (lds(qb + nbo[k][2] * sc8, 0.0) + lds(qb + nbo[k][3] * sc8, 0.0))) +
+                             (lds(qb + nbo[k][4] * sc8, 0.0) + lds(qb + nbo[k][5] * sc8, 0.0));
           const double rd = b64[k] - (double(dg[k]) * q[k] - acc);
           tm = dmax(tm, fabs(rd));
           rt[k] = T(rd);
         }
-        const double tres = reduce2(tm, 0.0, C, phase, me, ns, cl).x;
+        const double tres = reduce3(tm, 0.0, 0.0, C, rr, me, ns, ok).x;
         if (tres <= target) {
           res_norm = tres;
           converged = 1;
@@ -418,23 +627,30 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, 
         restarts++;
 #pragma unroll
         for (int k = 0; k < K; k++) r[k] = rt[k];
-        precondition(&zr, &rm);
-        sigma = reduce2(0.0, zr, C, phase, me, ns, cl).y;
+        precondition();
+        apply_z(&zr, &zw);
+        const double3 h3 = reduce3(0.0, zr, zw, C, rr, me, ns, ok);
+        gamma = h3.y;
+        delta = h3.z;
         fresh = true;
         continue;
       }
-      beta = both.y / sigma;
-      sigma = both.y;
+      gamma_prev = gamma;
+      gamma = g3.y;
+      delta = g3.z;
+      alpha_prev = alpha;
+      fresh = false;
     }
     iters = converged ? it : a.max_iter;
     if (!converged) converged = res_norm <= target ? 1 : 0;
   }
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    const int t = threadIdx.x + k * nt;
-    if (t < cnt) a.q[own0 + t] = q[k];
+    const int t = tid + k * nt;
+    if (has[k]) a.q[P.tperm[own0 + t]] = q[k];
   }
-  if (me == 0 && threadIdx.x == 0) {
+  if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);
+  if (me == 0 && tid == 0) {
     if (a.is_correction) {
       sc->corr_iters = iters;
       sc->corr_residual = res_norm;
@@ -445,20 +661,26 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS) k_chebpcg(Geo g, DevPtrs P, 
     }
     sc->mg_status = 1;
   }
-  cl.sync();  // no rank leaves while another may still write into its shared memory
+  cl.sync();  // no rank leaves while another may still address its shared memory
+  // after a wait gave up anywhere in the cluster, stores of skipped rounds may still be in flight:
+  // let them land before the shared memory is released
+  if (tid == 0 && (*reinterpret_cast<volatile int*>(&sc->errors) & ERR_SOLVER_TIMEOUT))
+    for (int i = 0; i < 100; i++) __nanosleep(10000);
 }
 
-void cheb_configure() {
-  cudaFuncSetAttribute(k_chebpcg<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHEB_SMEM);
-  cudaFuncSetAttribute(k_chebpcg<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHEB_SMEM);
-  cudaFuncSetAttribute(k_chebpcg<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  cudaFuncSetAttribute(k_chebpcg<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+namespace {
+
+template <typename T, int K>
+void configure_one() {
+  cudaFuncSetAttribute(k_chebpcg<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHEB_SMEM);
+  cudaFuncSetAttribute(k_chebpcg<T, K>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
-void launch_cheb_solve(const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st) {
+template <int K>
+void launch_k(const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(a.cluster);
-  cfg.blockDim = dim3(a.threads);
+  cfg.blockDim = dim3(std::min(a.threads, CHEB_MAX_THREADS / K));
   cfg.dynamicSmemBytes = a.smem_bytes;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -469,9 +691,46 @@ void launch_cheb_solve(const Geo& g, const DevPtrs& P, const SolverWs& W, const 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (a.mixed)
-    cudaLaunchKernelEx(&cfg, k_chebpcg<float>, g, P, W, a);
+    cudaLaunchKernelEx(&cfg, k_chebpcg<float, K>, g, P, W, a);
   else
-    cudaLaunchKernelEx(&cfg, k_chebpcg<double>, g, P, W, a);
+    cudaLaunchKernelEx(&cfg, k_chebpcg<double, K>, g, P, W, a);
+}
+
+void launch_cells(int K, const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st) {
+  if (K == 1)
+    launch_k<1>(g, P, W, a, st);
+  else if (K == 2)
+    launch_k<2>(g, P, W, a, st);
+  else
+    launch_k<4>(g, P, W, a, st);
+}
+
+// Cells the launch with K cells per thread can hold.
+int capacity(const ChebArgs& a, int K) { return a.cluster * std::min(a.threads, CHEB_MAX_THREADS / K) * K; }
+
+}  // namespace
+
+void cheb_configure() {
+  configure_one<double, 1>();
+  configure_one<double, 2>();
+  configure_one<double, 4>();
+  configure_one<float, 1>();
+  configure_one<float, 2>();
+  configure_one<float, 4>();
+}
+
+// The launch sized for a.m_bound liquid cells, then (gated on the device) one with four cells per
+// thread for a pour that exceeds it; the wavefront solver launched after these takes any system
+// neither could hold.
+void launch_cheb_solve(const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st) {
+  int K = 1;
+  while (K < CHEB_KMAX && capacity(a, K) < a.m_bound) K *= 2;
+  launch_cells(K, g, P, W, a, st);
+  if (K < CHEB_KMAX && capacity(a, CHEB_KMAX) > capacity(a, K)) {
+    ChebArgs b = a;
+    b.gate = 1;
+    launch_cells(CHEB_KMAX, g, P, W, b, st);
+  }
 }
 
 }  // namespace pl

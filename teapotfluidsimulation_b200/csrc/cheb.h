@@ -7,11 +7,11 @@
 namespace pl {
 
 constexpr int CHEB_CLUSTER = 16;       // largest cluster (non-portable size, one CTA per SM)
-constexpr int CHEB_MAX_THREADS = 512;  // largest CTA
-constexpr int CHEB_SMEM = 224 * 1024;  // dynamic shared memory per CTA
+constexpr int CHEB_MAX_THREADS = 1024;  // largest CTA
+constexpr int CHEB_SMEM = 220 * 1024;   // dynamic shared memory per CTA
 constexpr int CHEB_DEGREE = 12;        // polynomial degree (stencil applications per CG iteration)
 constexpr double CHEB_LO = 0.03;        // lower end of the D^-1 A interval the polynomial targets
-constexpr int CHEB_KMAX = 4;           // cells per thread whose state stays in registers
+constexpr int CHEB_KMAX = 4;           // most cells per thread (their state stays in registers)
 
 struct ChebArgs {
   const double* b;  // list-indexed rhs
@@ -23,8 +23,10 @@ struct ChebArgs {
   int degree;
   double cheb_lo;
   int cluster;     // CTAs in the cluster (launch shape, chosen by the tuner)
-  int threads;     // threads per CTA
+  int threads;     // threads per CTA (at most 1024 / cells per thread)
   int smem_bytes;  // dynamic shared memory per CTA
+  int m_bound;     // liquid cells the launch is sized for (cells per thread from it)
+  int gate;        // run only if the solve before it could not take the system (mg_status == 0)
 };
 
 void cheb_configure();

@@ -35,6 +35,14 @@ constexpr int SCAN_MAX_BINS = 4096 * 2048;
 // Error flags (SimScalars::errors).
 constexpr int ERR_SCAN_TIMEOUT = 1;
 constexpr int ERR_SOLVER_SIZE = 2;
+constexpr int ERR_SOLVER_TIMEOUT = 4;  // a cluster solve's bounded wait for a neighbour gave up
+
+// Column tiles of the cluster solver's cell order: the liquid cells sorted by (8 x 8 column tile,
+// k, j, i), so that contiguous ranges of that order are compact blocks. One 64-bit mask per
+// (tile, plane) marks the liquid cells; grids with more tile planes than TILE_PLANES_MAX keep the
+// list order.
+constexpr int TILE_W = 8;
+constexpr int TILE_PLANES_MAX = 8192;
 
 // Constant per simulation: grid, physics, pot geometry (vessel3d.ts:34-59, solver3d.ts:116-182).
 struct Geo {
@@ -51,6 +59,8 @@ struct Geo {
   int precision;
   int solve_cluster;  // launch shape of the cluster solves (set by the tuner)
   int solve_threads;
+  int ntx, nty;  // column tiles along x and y
+  int tiled;     // the cluster solver orders its cells by column tile (ntx * nty * nz <= TILE_PLANES_MAX)
   double parcel_volume;
   double R;  // Math.hypot(nx, ny) * h  (solver3d.ts:275)
   // teapot
@@ -254,6 +264,10 @@ struct DevPtrs {
   void* solver_ws;
   size_t solver_ws_bytes;
   void* mg_ws;  // multigrid hierarchy
+  // cluster solver order (positions in the column-tile order of the liquid cells)
+  unsigned long long* tile_mask;  // ntx * nty * nz masks of liquid cells, bit (j % 8) * 8 + i % 8
+  int* tnb;    // 6 * nc: tile-order position of the -x,+x,-y,+y,-z,+z liquid neighbour or -1
+  int* tperm;  // nc: liquid-list index of the cell at each tile-order position
   // render
   float* render;
   SimScalars* sc;

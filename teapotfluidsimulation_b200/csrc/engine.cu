@@ -79,8 +79,10 @@ int pull_scalars(pl_sim* s) {
   s->pending = 0;
   if (s->hs.errors) {
     int e = s->hs.errors;
-    return fail(PL_E_TIMEOUT, "device error flags 0x%x (%s%s)", e, (e & ERR_SCAN_TIMEOUT) ? "bin scan wait gave up " : "",
-                (e & ERR_SOLVER_SIZE) ? "solver wavefronts exceed capacity" : "");
+    return fail(PL_E_TIMEOUT, "device error flags 0x%x (%s%s%s)", e,
+                (e & ERR_SCAN_TIMEOUT) ? "bin scan wait gave up " : "",
+                (e & ERR_SOLVER_SIZE) ? "solver wavefronts exceed capacity " : "",
+                (e & ERR_SOLVER_TIMEOUT) ? "cluster solve wait gave up" : "");
   }
   return PL_OK;
 }
@@ -274,6 +276,8 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       N * 6 * 4,                                       // render
       sizeof(SimScalars), F * 4,                       // scalars, export
       mg_ws_bytes(g, nullptr),                         // multigrid hierarchy
+      size_t(g.ntx) * g.nty * g.nz * 8,                // column-tile masks
+      C * 6 * 4, C * 4,                                // tile-order neighbours, permutation
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -324,6 +328,9 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.sc = (SimScalars*)take();
   s->export_buf = (float*)take();
   P.mg_ws = take();
+  P.tile_mask = (unsigned long long*)take();
+  P.tnb = (int*)take();
+  P.tperm = (int*)take();
   mg_configure();
   cheb_configure();
   int nn = g.n;
@@ -415,8 +422,8 @@ int pl_autotune_solver(const pl_config* cfg, int32_t substeps, int32_t* best_clu
   if (!cfg || substeps < 1 || !best_cluster || !best_threads) return fail(PL_E_ARG, "pl_autotune_solver: bad argument");
   pl_config c = *cfg;
   c.preconditioner = PL_PRECOND_CHEB;
-  const int clusters[] = {16, 8, 12, 4};
-  const int threads[] = {256, 128, 512};
+  const int clusters[] = {16, 12, 8};
+  const int threads[] = {512, 1024, 256};
   float best = INFINITY;
   int bc = 0, bt = 0;
   for (int ci : clusters)

@@ -93,6 +93,7 @@ __global__ void k_bin_count(Geo g, DevPtrs P) {
   if (!P.sc->active) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < SCAN_MAX_TILES) P.scan_state[s] = 0ull;
+  if (g.tiled && s < g.ntx * g.nty * g.nz) P.tile_mask[s] = 0ull;
   if (s >= g.n) return;
   float4 p = P.pos_home[s];
   float4 v = P.vel_home[s];
@@ -160,7 +161,14 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       v = (unsigned long long)(unsigned)cn;
       if (b < g.nc) {
         typ[e] = classify_cell(g, sc, b, cn > 0);
-        if (typ[e] == FLUID) v += 1ull << 32;
+        if (typ[e] == FLUID) {
+          v += 1ull << 32;
+          if (g.tiled) {
+            const int i = b % g.nx, j = (b / g.nx) % g.ny, k = b / (g.nx * g.ny);
+            const int tp = ((j / TILE_W) * g.ntx + i / TILE_W) * g.nz + k;
+            atomicOr(&P.tile_mask[tp], 1ull << ((j % TILE_W) * TILE_W + i % TILE_W));
+          }
+        }
       }
     }
     val[e] = v;
@@ -759,7 +767,7 @@ static inline int blocks(int n, int t) { return (n + t - 1) / t; }
 
 void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_controller<<<1, 1, 0, st>>>(g, P);
-  k_bin_count<<<blocks(max(g.n, SCAN_MAX_TILES), 256), 256, 0, st>>>(g, P);
+  k_bin_count<<<blocks(max(max(g.n, SCAN_MAX_TILES), g.tiled ? g.ntx * g.nty * g.nz : 0), 256), 256, 0, st>>>(g, P);
   k_scan_classify<<<blocks(g.nbins, SCAN_TILE), SCAN_THREADS, 0, st>>>(g, P);
   k_bin_place<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
   k_bin_permute<<<blocks(g.n, 256), 256, 0, st>>>(g, P);

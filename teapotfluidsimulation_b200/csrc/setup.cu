@@ -169,9 +169,12 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
   g.max_iter = cfg.pressure_max_iterations;
   g.precond = cfg.preconditioner;
   g.precision = cfg.solve_precision;
+  g.ntx = (g.nx + TILE_W - 1) / TILE_W;
+  g.nty = (g.ny + TILE_W - 1) / TILE_W;
+  g.tiled = g.ntx * g.nty * g.nz <= TILE_PLANES_MAX ? 1 : 0;
   g.solve_cluster = cfg.solve_cluster > 0 ? cfg.solve_cluster : 16;
-  g.solve_threads = cfg.solve_threads > 0 ? cfg.solve_threads : 256;
-  if (g.solve_cluster > 16 || g.solve_threads < 32 || g.solve_threads > 512 || g.solve_threads % 32) {
+  g.solve_threads = cfg.solve_threads > 0 ? cfg.solve_threads : 512;
+  if (g.solve_cluster > 16 || g.solve_threads < 32 || g.solve_threads > 1024 || g.solve_threads % 32) {
     snprintf(err, errlen, "pl_create: solve shape %d x %d out of range", g.solve_cluster, g.solve_threads);
     return PL_E_ARG;
   }

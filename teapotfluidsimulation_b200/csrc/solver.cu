@@ -9,6 +9,7 @@
 // and every preconditioner application agree with the FP64 reference bit for bit. Inner products
 // are fixed-order tree reductions (deterministic; they differ from the reference's sequential sums
 // only in rounding).
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -55,21 +56,70 @@ size_t solver_ws_bytes(int cap) {
 // ---------------------------------------------------------------- setup (many blocks)
 
 // Neighbour list indices, diagonal, wavefront and the pressure rhs of every liquid cell
-// (solver3d.ts:869-881 and divergenceRhs, solver3d.ts:473-493).
-__global__ void k_solve_setup(Geo g, DevPtrs P, SolverWs W, int compute_rhs) {
+// (solver3d.ts:869-881 and divergenceRhs, solver3d.ts:473-493). With tile_order, also the cluster
+// solver's column-tile order: every block first forms the exclusive prefix of the (tile, plane)
+// mask populations in shared memory (dynamic, ntx * nty * nz <= TILE_PLANES_MAX ints); a liquid cell's position is then
+// its plane's prefix plus the liquid cells before it in its plane of the tile.
+__global__ void k_solve_setup(Geo g, DevPtrs P, SolverWs W, int compute_rhs, int tile_order) {
   const SimScalars* sc = P.sc;
   if (!sc->active) return;
+  extern __shared__ int s_pre[];
+  __shared__ int s_warp[32];
   const int m = sc->m;
   const int nxy = g.nx * g.ny;
+  const bool tiled = tile_order && g.tiled;
+  if (tiled) {
+    const int T = g.ntx * g.nty * g.nz;
+    const int per = (T + blockDim.x - 1) / blockDim.x;
+    const int e0 = threadIdx.x * per;
+    int sum = 0;
+    for (int q = 0; q < per; q++)
+      if (e0 + q < T) sum += __popcll(P.tile_mask[e0 + q]);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < nw; w++) {
+        int c = s_warp[w];
+        s_warp[w] = acc;
+        acc += c;
+      }
+    }
+    __syncthreads();
+    int run = s_warp[wid] + x - sum;
+    for (int q = 0; q < per; q++)
+      if (e0 + q < T) {
+        s_pre[e0 + q] = run;
+        run += __popcll(P.tile_mask[e0 + q]);
+      }
+    __syncthreads();
+  }
+  auto tpos = [&](int c) {
+    const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / nxy;
+    const int tp = ((j / TILE_W) * g.ntx + i / TILE_W) * g.nz + k;
+    const int bit = (j % TILE_W) * TILE_W + i % TILE_W;
+    return s_pre[tp] + __popcll(P.tile_mask[tp] & ((1ull << bit) - 1ull));
+  };
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
     int c = P.list[t];
     int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / nxy;
     const int off[6] = {-1, 1, -g.nx, g.nx, -nxy, nxy};
     double d = 0;
+    const int p = tiled ? tpos(c) : t;
+    if (tile_order) P.tperm[p] = t;
 #pragma unroll
     for (int e = 0; e < 6; e++) {
       int cc = c + off[e];
-      W.nb[e * W.cap + t] = P.lidx[cc];
+      const int li = P.lidx[cc];
+      W.nb[e * W.cap + t] = li;
+      if (tile_order) P.tnb[e * g.nc + p] = li < 0 ? -1 : (tiled ? tpos(cc) : li);
       if (P.cell[cc] != SOLID) d += 1;
     }
     W.adiag[t] = d;
@@ -404,13 +454,19 @@ __global__ void __launch_bounds__(SOLVER_THREADS) k_pcg(Geo g, DevPtrs P, Solver
 
 static SolverWs ws_of(const DevPtrs& P, int cap) { return solver_ws_carve(P.solver_ws, cap); }
 
+// Liquid cells a cluster solve is sized for: a quarter more than the parcels fill at the seeding
+// density of about 8 per cell (the liquid of a pour spreads, but it does not grow); a system above
+// it goes to a launch sized for more, then to the wavefront solver.
+static int cheb_m_bound(const Geo& g) { return std::min(g.nc, g.n * 5 / 32 + 64); }
+
 // Pressure solve (project(), solver3d.ts:530-543). With the multigrid preconditioner the cluster
 // solve runs first and the wavefront MIC(0) solve only if the cluster's shared memory could not
 // hold the hierarchy (it then factors as usual).
 void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   SolverWs W = ws_of(P, g.nc);
-  k_solve_setup<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, W, 1);
   const bool mg = g.precond == PL_PRECOND_MG, cheb = g.precond == PL_PRECOND_CHEB;
+  const size_t pre_bytes = (cheb && g.tiled) ? size_t(g.ntx) * g.nty * g.nz * 4 : 0;
+  k_solve_setup<<<DENSITY_BLOCKS, 256, pre_bytes, st>>>(g, P, W, 1, cheb ? 1 : 0);
   if (mg) {
     MgWs M = mg_ws_carve(g, P.mg_ws, P, W);
     launch_mg_setup(g, P, M, st);
@@ -418,7 +474,7 @@ void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   } else if (cheb) {
     launch_cheb_solve(g, P, W,
                       ChebArgs{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
-                               g.solve_cluster, g.solve_threads, CHEB_SMEM},
+                               g.solve_cluster, g.solve_threads, CHEB_SMEM, cheb_m_bound(g), 0},
                       st);
   }
   SolveArgs a{W.bp, P.q, g.tol, g.max_iter, 0, 1, (mg || cheb) ? 1 : 0};
@@ -434,7 +490,7 @@ void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
     launch_mg_solve(g, P, M, MgArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED}, st);
   } else if (cheb) {
     launch_cheb_solve(g, P, W, ChebArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
-                               g.solve_cluster, g.solve_threads, CHEB_SMEM},
+                               g.solve_cluster, g.solve_threads, CHEB_SMEM, cheb_m_bound(g), 0},
                       st);
   }
   SolveArgs a{P.rhs, P.qc, 1e-4, 80, 1, 0, (mg || cheb) ? 1 : 0};

@@ -70,7 +70,7 @@ def test_standalone_and_engine_agree_on_rerun(engine):
 def test_autotune_returns_a_working_shape(engine):
     cfg = abi.gentle_pour(10, 20)
     c, t, ms = engine.engine.autotune_solver(cfg, 2)
-    assert 1 <= c <= 16 and t in (128, 256, 512) and ms > 0
+    assert 1 <= c <= 16 and t in (256, 512, 1024) and ms > 0
     cfg.preconditioner = abi.PRECOND_CHEB
     cfg.solve_cluster, cfg.solve_threads = c, t
     sim = engine.Simulation3D(cfg)
