@@ -168,7 +168,7 @@ def measured_peaks():
 
 def profile_traffic():
     """DRAM bytes per launch of the pressure PCG kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "pcg_pressure_ncu.md")
+    path = os.path.join(ROOT, "profiles", "k_chebpcg_4mm_full.md")
     try:
         with open(path) as f:
             for line in f:
@@ -286,6 +286,7 @@ def run_ours(args):
     stage_acc: dict = {}
     pcg_work = 0.0
     iters = []
+    corr_iters = []
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -299,6 +300,7 @@ def run_ours(args):
         steps_done += 1
         d = sim.diagnostics()
         iters.append(d["pressureIterations"])
+        corr_iters.append(d["correctionIterations"])
         pcg_work += pcg_bytes_per_iteration(d["liquidCells"], args.precond, args.precision) * d["pressureIterations"]
     torch.cuda.synchronize()
     barrier(world)
@@ -342,6 +344,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "pressure_ms_per_substep": pres_ms,
         "pressure_iterations_mean": (sum(iters) / len(iters)) if iters else 0,
+        "correction_iterations_mean": (sum(corr_iters) / len(corr_iters)) if corr_iters else 0,
         "stages_ms_per_substep": {k: v / max(steps_done, 1) for k, v in stage_acc.items()},
         "gpu_launches": KERNELS_PER_SUBSTEP[args.precond] * steps_done,
         "e2e": {"value": e2e_value, "unit": "sim-s/wall-s", "h2d_bytes_per_step": scalars,
