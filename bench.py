@@ -31,9 +31,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "gentle 400 mL pour, 4 mm cells, half pot (81x81x22 grid, 88,856 parcels), seed 1"
-# kernels per substep: controller, bin count/scan/place/permute, p2g, solve setup, pressure solve,
+# kernels per substep: controller, bin count/scan/place/permute, p2g cells + faces, solve setup, pressure solve,
 # 2x extrapolation, density, correction solve, advect; the cluster solves add their gated fallback
-KERNELS_PER_SUBSTEP = {"mic0": 13, "cheb": 15, "mg": 16}
+KERNELS_PER_SUBSTEP = {"mic0": 14, "cheb": 16, "mg": 17}
 
 
 def parse():

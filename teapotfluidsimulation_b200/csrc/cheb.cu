@@ -55,6 +55,12 @@ constexpr int CHEB_BITMAP_WORDS = 1024;  // remote-reference bitmap over liquid 
 
 __device__ __forceinline__ uint32_t s_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Shared::cluster address of the same shared-memory location in CTA `rank`.
 __device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
   uint32_t o;
@@ -218,7 +224,8 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   SimScalars* sc = P.sc;
   if (!sc->active) return;
   if (a.gate && sc->mg_status) return;  // the launch before this one solved the system
-  if (a.is_correction) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->t_solve[0] = globaltimer_ns();
+  if (a.jobs == 1 && a.is_correction) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // interior mean of the density ratios (solver3d.ts:670)
       double s = 0;
       int n = 0;
@@ -425,23 +432,20 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     sv<uint32_t>(smem, DST, p * chunk + int(rq.x)) = rq.y;
   }
   __syncthreads();
-  // ---- per-thread state of the owned cells
+  // ---- per-thread state of the owned cells (the exchange data serves every job of the launch)
   T r[K], z[K], res[K], as[K], sown[K], cdown[K], idg[K], dg[K], w[K];
   double q[K], b64[K];
-  int nd[K];             // requesting ranks
+  int li_own[K];            // liquid-list index of each own cell
+  int nd[K];                // requesting ranks
   uint32_t d0a[K], d0b[K];  // the first one's halo slot (in its vector at offset 0) and exchange barrier
-  double bmax = 0;
 #pragma unroll
   for (int k = 0; k < K; k++) {
     const int t = tid + k * nt;
     const int li = has[k] ? P.tperm[own0 + t] : 0;
+    li_own[k] = li;
     const double d = has[k] ? W.adiag[li] : 1.0;
     dg[k] = T(d);
     idg[k] = T(1) / T(d);
-    b64[k] = has[k] ? a.b[li] : 0.0;
-    r[k] = T(b64[k]);
-    q[k] = 0;
-    z[k] = res[k] = as[k] = sown[k] = cdown[k] = w[k] = T(0);
     nd[k] = has[k] ? sv<int>(smem, DCNT, t) : 0;
     d0a[k] = d0b[k] = 0;
     if (nd[k] > 0) {
@@ -450,7 +454,6 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       d0a[k] = C.rsmem[rk] + uint32_t(guard + 1 + int(dd & 0xffffu)) * uint32_t(sizeof(T));
       d0b[k] = C.rxbar[rk];
     }
-    bmax = dmax(bmax, fabs(b64[k]));
   }
   const uint32_t sbase = s_addr(smem);
   const uint32_t xb0 = s_addr(&C.xbar[0]);
@@ -498,7 +501,6 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     const T x3 = lds(vb + nbo[k][3], T()), x4 = lds(vb + nbo[k][4], T()), x5 = lds(vb + nbo[k][5], T());
     return ((x0 + x1) + (x2 + x3)) + (x4 + x5);
   };
-  const double bnorm = reduce3(bmax, 0.0, 0.0, C, rr, me, ns, ok).x;
   const T itheta = T(2.0 / (2.0 + a.cheb_lo));
   // z = p(D^-1 A) D^-1 r, published (own cells and halo) in ZS
   auto precondition = [&]() {
@@ -548,10 +550,45 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     *zr = pr;
     *zw = pw;
   };
+  for (int job = 0; job < a.jobs; job++) {
+  // job 0: the launch's first system (pressure, or the one system of a single-job launch); job 1:
+  // the density correction of the same substep (same liquid cells, so the same exchange tables)
+  const bool corr = job == 1 || a.is_correction;
+  const double* jb = job == 0 ? a.b : a.b2;
+  double* jq = job == 0 ? a.q : a.q2;
+  const double jtol = job == 0 ? a.tol : a.tol2;
+  const int jmax = job == 0 ? a.max_iter : a.max_iter2;
+  if (job == 1) {
+    if (me == 0 && tid == 0) {  // interior mean of the density ratios (solver3d.ts:670)
+      sc->t_solve[1] = globaltimer_ns();
+      double s = 0;
+      int n = 0;
+      for (int b = 0; b < DENSITY_BLOCKS; b++) {
+        s += P.interior_part[b];
+        n += P.interior_cnt_part[b];
+      }
+      sc->interior = n > 0 ? s / n : 1.0;
+      sc->interior_count = n;
+    }
+    if (!sc->corr_any) {  // solver3d.ts:671: no solve, uc = vc = wc = 0 (uniform: set before the launch)
+      if (me == 0 && tid == 0) sc->corr_iters = 0;
+      break;
+    }
+  }
+  double bmax = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    b64[k] = has[k] ? jb[li_own[k]] : 0.0;
+    r[k] = T(b64[k]);
+    q[k] = 0;
+    z[k] = res[k] = as[k] = sown[k] = cdown[k] = w[k] = T(0);
+    bmax = dmax(bmax, fabs(b64[k]));
+  }
+  const double bnorm = reduce3(bmax, 0.0, 0.0, C, rr, me, ns, ok).x;
   int iters = 0, converged = 1;
   double res_norm = bnorm;
   if (m > 0 && !(bnorm < 1e-14)) {
-    const double target = dmax(a.tol * bnorm, 1e-14);
+    const double target = dmax(jtol * bnorm, 1e-14);
     converged = 0;
     int restarts = 0;
     bool fresh = true;
@@ -565,7 +602,7 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       delta = g3.z;
     }
     int it = 1;
-    for (; it <= a.max_iter; it++) {
+    for (; it <= jmax; it++) {
       double beta = 0, sas = delta;
       if (!fresh) {
         beta = gamma / gamma_prev;
@@ -641,17 +678,14 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       alpha_prev = alpha;
       fresh = false;
     }
-    iters = converged ? it : a.max_iter;
+    iters = converged ? it : jmax;
     if (!converged) converged = res_norm <= target ? 1 : 0;
   }
 #pragma unroll
-  for (int k = 0; k < K; k++) {
-    const int t = tid + k * nt;
-    if (has[k]) a.q[P.tperm[own0 + t]] = q[k];
-  }
-  if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);
+  for (int k = 0; k < K; k++)
+    if (has[k]) jq[li_own[k]] = q[k];
   if (me == 0 && tid == 0) {
-    if (a.is_correction) {
+    if (corr) {
       sc->corr_iters = iters;
       sc->corr_residual = res_norm;
     } else {
@@ -659,6 +693,13 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       sc->last_residual = res_norm;
       if (!converged) sc->failures++;
     }
+  }
+  }  // jobs
+  if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);
+  if (me == 0 && tid == 0) {
+    const unsigned long long t = globaltimer_ns();
+    sc->t_solve[2] = t;
+    if (a.jobs < 2 || !sc->corr_any) sc->t_solve[1] = t;
     sc->mg_status = 1;
   }
   cl.sync();  // no rank leaves while another may still address its shared memory

@@ -27,6 +27,13 @@ struct ChebArgs {
   int smem_bytes;  // dynamic shared memory per CTA
   int m_bound;     // liquid cells the launch is sized for (cells per thread from it)
   int gate;        // run only if the solve before it could not take the system (mg_status == 0)
+  // a second system on the same liquid cells, solved after the first in the same launch (jobs = 2):
+  // the density correction after the pressure
+  int jobs;
+  const double* b2;
+  double* q2;
+  double tol2;
+  int max_iter2;
 };
 
 void cheb_configure();

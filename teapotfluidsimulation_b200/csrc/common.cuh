@@ -111,6 +111,9 @@ struct SimScalars {
   int pad1;
   double last_residual;
   double corr_residual;
+  // globaltimer stamps (ns) of a two-system cluster solve: start, start of the correction system,
+  // end (the host splits the solve stage's event time into pressure and correction with them)
+  unsigned long long t_solve[3];
 };
 
 // ---------------------------------------------------------------- frames (solver3d.ts:232-260)
@@ -268,6 +271,13 @@ struct DevPtrs {
   unsigned long long* tile_mask;  // ntx * nty * nz masks of liquid cells, bit (j % 8) * 8 + i % 8
   int* tnb;    // 6 * nc: tile-order position of the -x,+x,-y,+y,-z,+z liquid neighbour or -1
   int* tperm;  // nc: liquid-list index of the cell at each tile-order position
+  // particle-to-grid node partials of this substep (cell-indexed, valid where occ[c] != 0):
+  // m_vel[(comp * 27 + slot) * nc + c] = (sum w, sum w v) of cell c's parcels for the comp-face node
+  // at offset slot = (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1) from the cell; m_den[slot * nc + c] =
+  // sum w for the cell-centred node at that offset (density)
+  uint8_t* occ;  // cell holds in-pot parcels
+  float2* m_vel;
+  float* m_den;
   // render
   float* render;
   SimScalars* sc;

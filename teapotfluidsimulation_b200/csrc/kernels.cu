@@ -2,20 +2,24 @@
 //
 // Order inside one substep (engine.cu builds it into a CUDA graph):
 //   k_controller      1 thread: stable dt, pour controller, pose (solver3d.ts:268-292)
-//   k_bin_count       parcels -> bin key (cell, or a removed-parcel bin) + atomic count
-//   k_scan_classify   one decoupled look-back scan over the bins: bin starts, cell types
-//                     (solver3d.ts:313-336), the liquid-cell list and its size
+//   k_bin_count       parcels -> bin key (cell, or a removed-parcel bin) + atomic count; cells ->
+//                     SOLID/AIR by the border and SDF test
+//   k_scan_classify   one decoupled look-back scan over the bins: bin starts, FLUID cells
+//                     (solver3d.ts:313-336), occupancy, the liquid-cell list and its size
 //   k_bin_place       parcels -> (id, slot) at start[key] + atomic rank
 //   k_bin_permute     canonical in-bin order by id, gather parcels into the sorted layout
-//   k_p2g             one thread per face: deterministic gather of the weighted sums over the
-//                     sorted parcels of the 18 neighbouring cells, normalise, gravity, wall
-//                     velocity, valid mask (solver3d.ts:410-471, 545-562)
-//   [pressure solve]  solver.cu
-//   k_grad_ext1       u -= grad q and the first extrapolation layer (solver3d.ts:496-528, 565-605)
+//   k_p2g_cells       one thread per (occupied cell, component): node partial sums of the cell's
+//                     parcels (velocity components and density)
+//   k_p2g             one thread per face: deterministic fixed-order sum of the partials of the
+//                     18 neighbouring cells, normalise, gravity, wall velocity, valid mask
+//                     (solver3d.ts:410-471, 545-562)
+//   k_density         density per liquid cell, correction rhs, interior statistics
+//                     (solver3d.ts:627-670): it depends only on the parcels and the cell types, so
+//                     it runs before the solves
+//   [pressure solve, correction solve]  solver.cu / cheb.cu (one cluster launch for both)
+//   k_grad_ext1       u -= grad q, the first extrapolation layer, max divergence after projection
+//                     (solver3d.ts:496-528, 565-605, 473-493)
 //   k_ext2            second extrapolation layer
-//   k_density         density per liquid cell, correction rhs, interior statistics, max
-//                     divergence (solver3d.ts:627-670, 473-493)
-//   [correction solve] solver.cu
 //   k_advect          FLIP/PIC grid-to-particle update, RK2 advection with the correction
 //                     velocity, SDF collision, symmetry plane, discharge and spill accounting
 //                     (solver3d.ts:607-624, 677-794)
@@ -89,11 +93,28 @@ __device__ __forceinline__ int parcel_bin(const Geo& g, float4 p, float4* frac, 
   return key;
 }
 
+// Solid part of the cell classification (solver3d.ts:313-322): border or inside the walls at the
+// current pose -> SOLID, else AIR; the scan then marks occupied non-solid cells FLUID. The SDF runs
+// in FP64 with the reference's operation order so the classification matches the FP64 reference
+// exactly.
+__device__ __forceinline__ uint8_t solid_or_air(const Geo& g, const SimScalars* sc, int c) {
+  int i = c % g.nx;
+  int j = (c / g.nx) % g.ny;
+  int k = c / (g.nx * g.ny);
+  if (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1) return SOLID;
+  double loc[3];
+  to_local(g, sc->c0, sc->s0, DMUL(i + 0.5, g.h), DMUL(j + 0.5, g.h), DMUL(k + 0.5, g.h), loc);
+  return teapot_sdf(g, loc[0], loc[1], loc[2]) < 0 ? SOLID : AIR;
+}
+
+// One thread per parcel and per cell: the parcel's bin key and rank in its bin, and the cell's solid
+// test (independent work in one launch so the SDF evaluations use the whole GPU).
 __global__ void k_bin_count(Geo g, DevPtrs P) {
   if (!P.sc->active) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < SCAN_MAX_TILES) P.scan_state[s] = 0ull;
   if (g.tiled && s < g.ntx * g.nty * g.nz) P.tile_mask[s] = 0ull;
+  if (s < g.nc) P.cell[s] = solid_or_air(g, P.sc, s);
   if (s >= g.n) return;
   float4 p = P.pos_home[s];
   float4 v = P.vel_home[s];
@@ -112,20 +133,6 @@ __global__ void k_bin_count(Geo g, DevPtrs P) {
   }
   P.key[s] = key;
   P.rank[s] = atomicAdd(&P.cnt[key], 1);
-}
-
-// Cell type (solver3d.ts:313-336): border or inside the walls at the current pose -> SOLID, else
-// FLUID when an in-pot parcel is in it, else AIR. The SDF runs in FP64 with the reference's
-// operation order so the classification matches the FP64 reference exactly.
-__device__ __forceinline__ uint8_t classify_cell(const Geo& g, const SimScalars* sc, int c, bool occupied) {
-  int i = c % g.nx;
-  int j = (c / g.nx) % g.ny;
-  int k = c / (g.nx * g.ny);
-  if (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1) return SOLID;
-  double loc[3];
-  to_local(g, sc->c0, sc->s0, DMUL(i + 0.5, g.h), DMUL(j + 0.5, g.h), DMUL(k + 0.5, g.h), loc);
-  if (teapot_sdf(g, loc[0], loc[1], loc[2]) < 0) return SOLID;
-  return occupied ? FLUID : AIR;
 }
 
 // Scan descriptors: bit 62-63 flag (1 aggregate, 2 inclusive prefix), bits 32-61 liquid cells,
@@ -160,7 +167,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       P.cnt[b] = 0;
       v = (unsigned long long)(unsigned)cn;
       if (b < g.nc) {
-        typ[e] = classify_cell(g, sc, b, cn > 0);
+        const uint8_t base = P.cell[b];  // SOLID or AIR from k_bin_count (solver3d.ts:313-336)
+        typ[e] = base == SOLID ? SOLID : cn > 0 ? FLUID : AIR;
         if (typ[e] == FLUID) {
           v += 1ull << 32;
           if (g.tiled) {
@@ -195,32 +203,48 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
   __syncthreads();
   unsigned long long thread_excl = x - local + (warp > 0 ? s_warp[warp - 1] : 0ull);
   unsigned long long aggregate = s_warp[SCAN_THREADS / 32 - 1];
-  // decoupled look-back (bounded waits)
-  if (threadIdx.x == 0) {
+  // decoupled look-back (bounded waits), one warp reading 32 predecessor descriptors at a time: the
+  // exclusive prefix is the sum of the aggregates back to the nearest inclusive prefix
+  if (warp == 0) {
     unsigned long long* desc = P.scan_state;
     if (tile == 0) {
-      atomicExch(&desc[0], DESC_INC | aggregate);
-      s_prefix = 0;
+      if (lane == 0) {
+        atomicExch(&desc[0], DESC_INC | aggregate);
+        s_prefix = 0;
+      }
     } else {
-      atomicExch(&desc[tile], DESC_AGG | aggregate);
+      if (lane == 0) atomicExch(&desc[tile], DESC_AGG | aggregate);
       unsigned long long excl = 0;
-      int j = tile - 1;
+      int top = tile - 1;  // highest predecessor not yet summed
       int spins = 0;
-      while (j >= 0) {
-        unsigned long long d = ld_volatile_u64(&desc[j]);
-        if ((d >> 62) == 0) {
+      bool failed = false;
+      while (top >= 0) {
+        const int j = top - lane;
+        const unsigned long long d = j >= 0 ? ld_volatile_u64(&desc[j]) : DESC_INC;  // below tile 0: prefix 0
+        // nearest predecessor (lowest lane) holding an inclusive prefix; the lanes up to it are needed
+        const unsigned inc = __ballot_sync(0xffffffffu, (d >> 62) == 2);
+        const unsigned pend = __ballot_sync(0xffffffffu, (d >> 62) == 0);
+        const int first = inc ? __ffs(inc) - 1 : 31;
+        const unsigned need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if (pend & need) {  // a needed descriptor is not published yet
           if (++spins > SPIN_LIMIT) {
-            atomicOr(&sc->errors, ERR_SCAN_TIMEOUT);
+            failed = true;
             break;
           }
           continue;
         }
-        excl += d & DESC_VAL;
-        if ((d >> 62) == 2) break;
-        j--;
+        unsigned long long v = lane <= first ? (d & DESC_VAL) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (inc) break;
+        top -= 32;
       }
-      atomicExch(&desc[tile], DESC_INC | (excl + aggregate));
-      s_prefix = excl;
+      if (lane == 0) {
+        if (failed) atomicOr(&sc->errors, ERR_SCAN_TIMEOUT);
+        atomicExch(&desc[tile], DESC_INC | (excl + aggregate));
+        s_prefix = excl;
+      }
     }
   }
   __syncthreads();
@@ -233,6 +257,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       if (b < g.nc) {
         int lpos = (int)((run >> 32) & 0x3fffffffull);
         P.cell[b] = typ[e];
+        P.occ[b] = (val[e] & 0xffffffffull) != 0 ? 1 : 0;
         if (typ[e] == FLUID) {
           P.list[lpos] = b;
           P.lidx[b] = lpos;
@@ -274,55 +299,159 @@ __global__ void k_bin_permute(Geo g, DevPtrs P) {
 
 // ---------------------------------------------------------------- particle-to-grid
 
-// Weight along one axis of a parcel in cell `cell` with FP64-derived fraction f for a node at
-// `node`; offset 0 (face axis) or 1/2 (cell-centred axis) as in solver3d.ts:352-360.
-__device__ __forceinline__ double axis_weight(int node, int cell, float f, bool half) {
-  int base = cell;
-  double fr = f;
-  if (half) {
-    if (f >= 0.5f) {
-      fr = (double)f - 0.5;
-    } else {
-      base = cell - 1;
-      fr = (double)f + 0.5;
-    }
+// Weights along one axis of a parcel with FP64-derived cell fraction f for the nodes at offsets -1,
+// 0, +1 from its cell: on a face axis (offset 0) the nodes 0 and +1; on a cell-centred axis (offset
+// 1/2) the nodes (-1, 0) or (0, +1) by which half of the cell the parcel is in (solver3d.ts:352-360).
+// Nodes the parcel does not touch get weight 0.
+__device__ __forceinline__ void axis_w3(float f, bool half, double w[3]) {
+  if (!half) {
+    w[0] = 0.0;
+    w[1] = 1.0 - (double)f;
+    w[2] = (double)f;
+  } else if (f >= 0.5f) {
+    const double fr = (double)f - 0.5;
+    w[0] = 0.0;
+    w[1] = 1.0 - fr;
+    w[2] = fr;
+  } else {
+    const double fr = (double)f + 0.5;
+    w[0] = 1.0 - fr;
+    w[1] = fr;
+    w[2] = 0.0;
   }
-  int d = node - base;
-  return d == 0 ? 1.0 - fr : d == 1 ? fr : -1.0;
 }
 
+// Node partials of one cell: for every node a parcel of the cell can touch, the sum over the cell's
+// parcels (in their canonical order) of the trilinear weight w = wx * wy * wz and of w times the
+// velocity component (COMP 0..2, particlesToGrid, solver3d.ts:410-431), or of w alone (COMP 3, the
+// density of densityCorrection, solver3d.ts:633-642). A node's full sum is then a fixed-order sum of
+// at most 18 (velocity) or 27 (density) partials, so the face and density gathers issue independent
+// loads instead of walking every parcel of the neighbourhood.
+template <int COMP>
+__device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int c, int p0, int p1) {
+  constexpr bool hx = COMP != 0, hy = COMP != 1, hz = COMP != 2;
+  double sw[27], swv[27];
+#pragma unroll
+  for (int q = 0; q < 27; q++) sw[q] = swv[q] = 0.0;
+  for (int p = p0; p < p1; p++) {
+    const float4 fr = P.frac_sorted[p];
+    double v = 0.0;
+    if (COMP < 3) v = (double)reinterpret_cast<const float*>(&P.vel_sorted[p])[COMP];
+    double wx[3], wy[3], wz[3];
+    axis_w3(fr.x, hx, wx);
+    axis_w3(fr.y, hy, wy);
+    axis_w3(fr.z, hz, wz);
+#pragma unroll
+    for (int ox = 0; ox < 3; ox++) {
+      if (!hx && ox == 0) continue;
+#pragma unroll
+      for (int oy = 0; oy < 3; oy++) {
+        if (!hy && oy == 0) continue;
+#pragma unroll
+        for (int oz = 0; oz < 3; oz++) {
+          if (!hz && oz == 0) continue;
+          const int q = ox * 9 + oy * 3 + oz;
+          const double w = wx[ox] * wy[oy] * wz[oz];
+          sw[q] += w;
+          if (COMP < 3) swv[q] += w * v;
+        }
+      }
+    }
+  }
+  const size_t nc = (size_t)g.nc;
+#pragma unroll
+  for (int q = 0; q < 27; q++) {
+    const int ox = q / 9, oy = (q / 3) % 3, oz = q % 3;
+    if ((!hx && ox == 0) || (!hy && oy == 0) || (!hz && oz == 0)) continue;
+    if (COMP < 3)
+      P.m_vel[((size_t)COMP * 27 + q) * nc + c] = make_float2((float)sw[q], (float)swv[q]);
+    else
+      P.m_den[(size_t)q * nc + c] = (float)sw[q];
+  }
+}
+
+// One thread per (occupied cell, component); blockIdx.y is the component (3 = density).
+__global__ void k_p2g_cells(Geo g, DevPtrs P) {
+  if (!P.sc->active) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.nc) return;
+  const int p0 = P.start[c], p1 = P.start[c + 1];
+  if (p0 == p1) return;
+  switch (blockIdx.y) {
+    case 0: cell_moments<0>(g, P, c, p0, p1); break;
+    case 1: cell_moments<1>(g, P, c, p0, p1); break;
+    case 2: cell_moments<2>(g, P, c, p0, p1); break;
+    default: cell_moments<3>(g, P, c, p0, p1); break;
+  }
+}
+
+// Weighted sums at face (i, j, k) of component COMP: the partials of the source cells at offsets
+// o = node - cell (face axis {0, 1}, others {-1, 0, 1}), interior cells only, in a fixed order. The
+// 18 occupancy loads are issued together, then the partials of the occupied cells as predicated
+// loads, so the loads overlap instead of waiting on one another.
+template <int COMP>
+__device__ __forceinline__ void face_sums(const Geo& g, const DevPtrs& P, int i, int j, int k, double* sw,
+                                          double* swv) {
+  constexpr int NX = COMP == 0 ? 2 : 3, NY = COMP == 1 ? 2 : 3, NZ = COMP == 2 ? 2 : 3;
+  constexpr int NS = NX * NY * NZ;
+  const size_t nc = (size_t)g.nc;
+  float2 m[NS];
+  bool use[NS];
+  size_t idx[NS];
+#pragma unroll
+  for (int z = 0; z < NZ; z++) {
+    const int oz = 1 - z;
+    const int cz = k - oz;
+    const bool inz = cz >= 1 && cz <= g.nz - 2;
+    const int czc = min(max(cz, 1), g.nz - 2);
+#pragma unroll
+    for (int y = 0; y < NY; y++) {
+      const int oy = 1 - y;
+      const int cy = j - oy;
+      const bool iny = cy >= 1 && cy <= g.ny - 2;
+      const int cyc = min(max(cy, 1), g.ny - 2);
+#pragma unroll
+      for (int x = 0; x < NX; x++) {
+        const int ox = 1 - x;
+        const int cx = i - ox;
+        const bool inx = cx >= 1 && cx <= g.nx - 2;
+        const int cxc = min(max(cx, 1), g.nx - 2);
+        const int c = cxc + g.nx * (cyc + g.ny * czc);
+        const int q = (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1);
+        const int e = (z * NY + y) * NX + x;
+        use[e] = inx && iny && inz && P.occ[c] != 0;
+        idx[e] = ((size_t)COMP * 27 + q) * nc + c;
+      }
+    }
+  }
+  // predicated loads: only occupied cells' partials are read (the others were never written)
+#pragma unroll
+  for (int e = 0; e < NS; e++) m[e] = use[e] ? P.m_vel[idx[e]] : make_float2(0.f, 0.f);
+  double a = 0.0, b = 0.0;
+#pragma unroll
+  for (int e = 0; e < NS; e++) {
+    a += use[e] ? (double)m[e].x : 0.0;
+    b += use[e] ? (double)m[e].y : 0.0;
+  }
+  *sw = a;
+  *swv = b;
+}
+
+// One thread per face: weighted average of the parcel velocities, gravity, wall velocity and valid
+// mask (solver3d.ts:410-471, 545-562).
 __global__ void k_p2g(Geo g, DevPtrs P) {
   const SimScalars* sc = P.sc;
   if (!sc->active) return;
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= g.nf) return;
   Face F = decode_face(g, f);
-  const int fc[3] = {F.i, F.j, F.k};
-  const int nn[3] = {g.nx, g.ny, g.nz};
-  int lo[3], hi[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    lo[a] = max(fc[a] - 1, 1);
-    hi[a] = min(a == F.comp ? fc[a] : fc[a] + 1, nn[a] - 2);
-  }
-  double sw = 0, swv = 0;
-  for (int cz = lo[2]; cz <= hi[2]; cz++)
-    for (int cy = lo[1]; cy <= hi[1]; cy++)
-      for (int cx = lo[0]; cx <= hi[0]; cx++) {
-        int c = cx + g.nx * (cy + g.ny * cz);
-        int p0 = P.start[c], p1 = P.start[c + 1];
-        for (int p = p0; p < p1; p++) {
-          float4 fr = P.frac_sorted[p];
-          double wx = axis_weight(F.i, cx, fr.x, F.comp != 0);
-          double wy = axis_weight(F.j, cy, fr.y, F.comp != 1);
-          double wz = axis_weight(F.k, cz, fr.z, F.comp != 2);
-          if (wx < 0 || wy < 0 || wz < 0) continue;
-          double w = wx * wy * wz;
-          const float* vel = reinterpret_cast<const float*>(&P.vel_sorted[p]);
-          sw += w;
-          swv += w * (double)vel[F.comp];
-        }
-      }
+  double sw, swv;
+  if (F.comp == 0)
+    face_sums<0>(g, P, F.i, F.j, F.k, &sw, &swv);
+  else if (F.comp == 1)
+    face_sums<1>(g, P, F.i, F.j, F.k, &sw, &swv);
+  else
+    face_sums<2>(g, P, F.i, F.j, F.k, &sw, &swv);
   double val = sw > 1e-9 ? swv / sw : 0.0;  // solver3d.ts:429
   P.uprev[f] = (float)val;
   // cells on the two sides of the face
@@ -370,11 +499,17 @@ __device__ __forceinline__ double projected(const Geo& g, const DevPtrs& P, int 
   return (double)P.u[f] + grad_term(g, P, P.q, comp, i, j, k);
 }
 
-__global__ void k_grad_ext1(Geo g, DevPtrs P) {
-  if (!P.sc->active) return;
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= g.nf) return;
-  Face F = decode_face(g, f);
+// |divergence| of liquid cell (i, j, k) after projection (divergenceRhs on the projected faces,
+// solver3d.ts:473-493, 542): the six face velocities with the gradient applied.
+__device__ __forceinline__ double projected_div(const Geo& g, const DevPtrs& P, int i, int j, int k) {
+  const int ux = g.nx + 1, vy = g.ny + 1;
+  const double d = (projected(g, P, 0, i + 1, j, k, ux, g.ny) - projected(g, P, 0, i, j, k, ux, g.ny)) +
+                   (projected(g, P, 1, i, j + 1, k, g.nx, vy) - projected(g, P, 1, i, j, k, g.nx, vy)) +
+                   (projected(g, P, 2, i, j, k + 1, g.nx, g.ny) - projected(g, P, 2, i, j, k, g.nx, g.ny));
+  return fabs(d);
+}
+
+__device__ __forceinline__ void grad_ext1_face(const Geo& g, const DevPtrs& P, int f, const Face& F) {
   if (P.valid[f]) {
     P.uext[f] = (float)projected(g, P, F.comp, F.i, F.j, F.k, F.sx, F.sy);
     P.vext[f] = 1;
@@ -400,6 +535,27 @@ __global__ void k_grad_ext1(Geo g, DevPtrs P) {
     P.uext[f] = P.u[f];
     P.vext[f] = 0;
   }
+}
+
+// Gradient update and first extrapolation layer per face; the u-face threads whose +x cell is liquid
+// also measure that cell's divergence after projection (max over cells, one atomic per warp).
+__global__ void k_grad_ext1(Geo g, DevPtrs P) {
+  SimScalars* sc = P.sc;
+  if (!sc->active) return;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bits = 0ull;
+  if (f < g.nf) {
+    const Face F = decode_face(g, f);
+    if (F.comp == 0 && F.i < g.nx && P.cell[F.i + g.nx * (F.j + g.ny * F.k)] == FLUID)
+      bits = (unsigned long long)__double_as_longlong(projected_div(g, P, F.i, F.j, F.k));
+    grad_ext1_face(g, P, f, F);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = ob > bits ? ob : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits) atomicMax(&sc->max_div_bits, bits);
 }
 
 __global__ void k_ext2(Geo g, DevPtrs P) {
@@ -437,27 +593,43 @@ __global__ void __launch_bounds__(256) k_density(Geo g, DevPtrs P) {
   double isum = 0;
   int icnt = 0;
   int any = 0;
-  double maxd = 0;
   const int nxy = g.nx * g.ny;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
     int c = P.list[t];
     int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / nxy;
-    // density: trilinear weights of parcels in the 27 neighbouring cells (solver3d.ts:633-642)
-    double dens = 0;
-    for (int cz = max(k - 1, 1); cz <= min(k + 1, g.nz - 2); cz++)
-      for (int cy = max(j - 1, 1); cy <= min(j + 1, g.ny - 2); cy++)
-        for (int cx = max(i - 1, 1); cx <= min(i + 1, g.nx - 2); cx++) {
-          int cc = cx + g.nx * (cy + g.ny * cz);
-          int p0 = P.start[cc], p1 = P.start[cc + 1];
-          for (int p = p0; p < p1; p++) {
-            float4 fr = P.frac_sorted[p];
-            double wx = axis_weight(i, cx, fr.x, true);
-            double wy = axis_weight(j, cy, fr.y, true);
-            double wz = axis_weight(k, cz, fr.z, true);
-            if (wx < 0 || wy < 0 || wz < 0) continue;
-            dens += wx * wy * wz;
-          }
+    // density: trilinear weights of the parcels of the 27 neighbouring cells (solver3d.ts:633-642),
+    // summed from the node partials of those cells in a fixed order (occupancy loads together, then
+    // predicated loads of the occupied cells' partials)
+    float dv[27];
+    bool du[27];
+    size_t di[27];
+#pragma unroll
+    for (int z = 0; z < 3; z++) {
+      const int oz = 1 - z, cz = k - oz;
+      const bool inz = cz >= 1 && cz <= g.nz - 2;
+      const int czc = min(max(cz, 1), g.nz - 2);
+#pragma unroll
+      for (int y = 0; y < 3; y++) {
+        const int oy = 1 - y, cy = j - oy;
+        const bool iny = cy >= 1 && cy <= g.ny - 2;
+        const int cyc = min(max(cy, 1), g.ny - 2);
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+          const int ox = 1 - x, cx = i - ox;
+          const bool inx = cx >= 1 && cx <= g.nx - 2;
+          const int cxc = min(max(cx, 1), g.nx - 2);
+          const int cc = cxc + g.nx * (cyc + g.ny * czc);
+          const int e = (z * 3 + y) * 3 + x;
+          du[e] = inx && iny && inz && P.occ[cc] != 0;
+          di[e] = (size_t)((ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)) * g.nc + cc;
         }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 27; e++) dv[e] = du[e] ? P.m_den[di[e]] : 0.f;
+    double dens = 0;
+#pragma unroll
+    for (int e = 0; e < 27; e++) dens += du[e] ? (double)dv[e] : 0.0;
     P.density[t] = dens;
     double ratio = dens / 8;
     const uint8_t* cl = P.cell;
@@ -473,27 +645,20 @@ __global__ void __launch_bounds__(256) k_density(Geo g, DevPtrs P) {
       any = 1;
     }
     P.rhs[t] = r;
-    // divergence after projection (solver3d.ts:473-493, 542)
-    const float* u = P.u;
-    int iu = i + (g.nx + 1) * (j + g.ny * k);
-    int iv = g.nu + i + g.nx * (j + (g.ny + 1) * k);
-    int iw = g.nu + g.nv + c;
-    double d = (double)u[iu + 1] - (double)u[iu] + (double)u[iv + g.nx] - (double)u[iv] + (double)u[iw + nxy] -
-               (double)u[iw];
-    maxd = dmax(maxd, fabs(d));
   }
-  // deterministic per-block partial sums (fixed shuffle tree, then warps in order)
+  // deterministic per-block partial sums (fixed shuffle tree, then warps in order); the flag is folded
+  // per warp so that one atomic per warp reaches the scalar block
   for (int o = 16; o > 0; o >>= 1) {
     isum += __shfl_down_sync(0xffffffffu, isum, o);
     icnt += __shfl_down_sync(0xffffffffu, icnt, o);
   }
+  any = __any_sync(0xffffffffu, any != 0) ? 1 : 0;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
     s_sum[warp] = isum;
     s_cnt[warp] = icnt;
+    if (any) atomicOr(&sc->corr_any, 1);
   }
-  if (any) atomicOr(&sc->corr_any, 1);
-  if (maxd > 0) atomicMax(&sc->max_div_bits, (unsigned long long)__double_as_longlong(maxd));
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0;
@@ -591,11 +756,9 @@ __device__ __forceinline__ void set_status(SimScalars* sc, int from, int to) {  
   atomicAdd(&sc->counts[to], 1);
 }
 
-__global__ void k_advect(Geo g, DevPtrs P) {
-  SimScalars* sc = P.sc;
-  if (!sc->active) return;
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.n) return;
+// One parcel's grid-to-particle update and advection; returns the FP64 bits of its |v|^2 when it
+// stays in the pot (the stableDt input of the next substep), else 0.
+__device__ __forceinline__ unsigned long long advect_one(const Geo& g, const DevPtrs& P, SimScalars* sc, int p) {
   float4 pos = P.pos_sorted[p];
   float4 vel = P.vel_sorted[p];
   int meta = __float_as_int(vel.w);
@@ -611,12 +774,12 @@ __global__ void k_advect(Geo g, DevPtrs P) {
     }
     P.pos_home[p] = pos;
     P.vel_home[p] = vel;
-    return;
+    return 0ull;
   }
   if (st != IN_POT) {
     P.pos_home[p] = pos;
     P.vel_home[p] = vel;
-    return;
+    return 0ull;
   }
   const double x0 = pos.x, y0 = pos.y, z0 = pos.z;
   double vx = vel.x, vy = vel.y, vz = vel.z;
@@ -694,7 +857,7 @@ __global__ void k_advect(Geo g, DevPtrs P) {
     vel.w = __int_as_float((meta & ~0xff) | LOST);
     P.pos_home[p] = pos;
     P.vel_home[p] = vel;
-    return;
+    return 0ull;
   }
   pos.x = (float)x1;
   pos.y = (float)y1;
@@ -726,12 +889,31 @@ __global__ void k_advect(Geo g, DevPtrs P) {
     if (new_st == DISCHARGED) atomicAdd(&sc->by_origin[(meta >> 8) & 0xff], 1);
     vel.w = __int_as_float((meta & ~0xff) | new_st);
   } else {
-    double sp = vx * vx + vy * vy + vz * vz;  // stableDt (solver3d.ts:269-274) of the next substep
-    atomicMax(&sc->max_speed_bits, (unsigned long long)__double_as_longlong(sp));
+    const double sp = vx * vx + vy * vy + vz * vz;  // stableDt (solver3d.ts:269-274) of the next substep
+    P.pos_home[p] = pos;
+    P.vel_home[p] = vel;
+    return (unsigned long long)__double_as_longlong(sp);
   }
   P.pos_home[p] = pos;
   P.vel_home[p] = vel;
+  return 0ull;
 }
+
+// The maximum speed is folded per warp (bit patterns of non-negative doubles order like the values),
+// so one atomic per warp reaches the scalar block instead of one per parcel.
+__global__ void __launch_bounds__(256, 2) k_advect(Geo g, DevPtrs P) {
+  SimScalars* sc = P.sc;
+  if (!sc->active) return;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bits = p < g.n ? advect_one(g, P, sc, p) : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = ob > bits ? ob : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits) atomicMax(&sc->max_speed_bits, bits);
+}
+
 
 // ---------------------------------------------------------------- render positions
 
@@ -767,13 +949,15 @@ static inline int blocks(int n, int t) { return (n + t - 1) / t; }
 
 void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_controller<<<1, 1, 0, st>>>(g, P);
-  k_bin_count<<<blocks(max(max(g.n, SCAN_MAX_TILES), g.tiled ? g.ntx * g.nty * g.nz : 0), 256), 256, 0, st>>>(g, P);
+  k_bin_count<<<blocks(max(max(max(g.n, g.nc), SCAN_MAX_TILES), g.tiled ? g.ntx * g.nty * g.nz : 0), 256), 256, 0,
+                st>>>(g, P);
   k_scan_classify<<<blocks(g.nbins, SCAN_TILE), SCAN_THREADS, 0, st>>>(g, P);
   k_bin_place<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
   k_bin_permute<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
 }
 
 void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+  k_p2g_cells<<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
 }
 

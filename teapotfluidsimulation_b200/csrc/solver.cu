@@ -472,27 +472,30 @@ void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
     launch_mg_setup(g, P, M, st);
     launch_mg_solve(g, P, M, MgArgs{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED}, st);
   } else if (cheb) {
-    launch_cheb_solve(g, P, W,
-                      ChebArgs{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
-                               g.solve_cluster, g.solve_threads, CHEB_SMEM, cheb_m_bound(g), 0},
-                      st);
+    // both systems of the substep in one cluster launch: the density-correction rhs depends only on
+    // the parcels and the cell types, so it is ready before the pressure solve
+    ChebArgs c{W.bp, P.q, g.tol, g.max_iter, 0, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
+               g.solve_cluster, g.solve_threads, CHEB_SMEM, cheb_m_bound(g), 0};
+    c.jobs = 2;
+    c.b2 = P.rhs;
+    c.q2 = P.qc;
+    c.tol2 = 1e-4;  // solver3d.ts:673
+    c.max_iter2 = 80;
+    launch_cheb_solve(g, P, W, c, st);
   }
   SolveArgs a{W.bp, P.q, g.tol, g.max_iter, 0, 1, (mg || cheb) ? 1 : 0};
   k_pcg<<<1, SOLVER_THREADS, 0, st>>>(g, P, W, a);
 }
 
-// Density-correction solve (solver3d.ts:671-674): tolerance 1e-4, at most 80 iterations.
+// Density-correction solve (solver3d.ts:671-674): tolerance 1e-4, at most 80 iterations. Runs after
+// the pressure solve; its rhs (k_density) is computed before the pressure solve.
 void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   SolverWs W = ws_of(P, g.nc);
   const bool mg = g.precond == PL_PRECOND_MG, cheb = g.precond == PL_PRECOND_CHEB;
   if (mg) {
     MgWs M = mg_ws_carve(g, P.mg_ws, P, W);
     launch_mg_solve(g, P, M, MgArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED}, st);
-  } else if (cheb) {
-    launch_cheb_solve(g, P, W, ChebArgs{P.rhs, P.qc, 1e-4, 80, 1, g.precision == PL_SOLVE_MIXED, CHEB_DEGREE, CHEB_LO,
-                               g.solve_cluster, g.solve_threads, CHEB_SMEM, cheb_m_bound(g), 0},
-                      st);
-  }
+  }  // the Chebyshev path solved this system in the pressure launch; only its fallback is left here
   SolveArgs a{P.rhs, P.qc, 1e-4, 80, 1, 0, (mg || cheb) ? 1 : 0};
   k_pcg<<<1, SOLVER_THREADS, 0, st>>>(g, P, W, a);
 }
