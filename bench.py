@@ -44,7 +44,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cell-mm", type=float, default=4.0)
     ap.add_argument("--precond", default="cheb", choices=["mic0", "mg", "cheb"])
-    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"],
+                    help="solver vectors: mixed = FP32 stencils/Chebyshev with FP64 inner products and FP64 "
+                         "true-residual refinement; f64 = all FP64")
     ap.add_argument("--start", type=float, default=0.0, help="simulated seconds to advance before warm-up")
     ap.add_argument("--cpu-sample", type=int, default=60, help="substeps of the CPU baseline sample")
     return ap.parse_args()
@@ -337,7 +339,8 @@ def run_ours(args):
     line = {
         "metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s", "n_gpus": world, "steps": steps_done,
         "warmup": args.warmup, "ms_per_step": max_ms / max(steps_done, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve / f32 parcels and faces", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": ("f32 solve vectors, f64 inner products/refinement" if args.precision == "mixed" else "f64 solve")
+                 + " / f32 parcels and faces, f64 transfer weights", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "preconditioner": args.precond,
                    "solve_precision": args.precision,
                    "start_s": args.start, "simulated_s": sim_s, "l2": "256 MiB buffer written between substeps",

@@ -486,11 +486,13 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   };
   // End of an exchange round of values of vbytes bytes: own values visible to the CTA, every halo
   // slot received.
+  // Warp 0 alone polls the barrier; the CTA barrier after it then orders every thread's reads of the
+  // round's own values and received halo values after both (cheaper than 16 warps polling).
   auto round_end = [&](uint32_t vbytes) {
     const uint32_t bar = xb0 + uint32_t(e & 1) * 8u;
     if (tid == 0) mbar_expect(bar, uint32_t(nh) * vbytes);
+    if (tid < 32) mbar_wait(bar, uint32_t(e >> 1) & 1u, ok);
     __syncthreads();
-    mbar_wait(bar, uint32_t(e >> 1) & 1u, ok);
     e++;
   };
   // Sum of the six neighbour values of own cell k in the vector at byte offset voff (pairwise: three
@@ -695,7 +697,7 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     }
   }
   }  // jobs
-  if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);
+  if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);  // (exchange waits run in warp 0)
   if (me == 0 && tid == 0) {
     const unsigned long long t = globaltimer_ns();
     sc->t_solve[2] = t;

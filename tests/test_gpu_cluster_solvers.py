@@ -80,11 +80,14 @@ def test_autotune_returns_a_working_shape(engine):
 
 
 @pytest.mark.slow
-def test_whole_pour_4mm_against_reference(engine, goldens):
-    # benchmarks/run3d.json 4 mm: 410.54 mL, shares 29.22 / 50.96 / 19.82 %
+@pytest.mark.parametrize("precision", [abi.SOLVE_F64, abi.SOLVE_MIXED])
+def test_whole_pour_4mm_against_reference(engine, goldens, precision):
+    # benchmarks/run3d.json 4 mm: 410.54 mL, shares 29.22 / 50.96 / 19.82 %; MIXED (FP32 vectors, FP64
+    # inner products and true-residual refinement) is the benchmarked configuration
     ref = {r["cellMm"]: r for r in goldens["run3d"]}[4]
     cfg = abi.gentle_pour(4, 20)
     cfg.preconditioner = abi.PRECOND_CHEB
+    cfg.solve_precision = precision
     sim = engine.Simulation3D(cfg)
     done_at = -1.0
     while not sim.finished:  # benchmarks/run3d.ts:14-23
