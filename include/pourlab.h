@@ -345,6 +345,46 @@ int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q,
                                 int32_t ny, int32_t nz, double tol, int32_t max_iter, void* stream,
                                 int32_t* iterations, int32_t* converged, double* residual);
 
+/* ------------------------------------------------------------------ Poisson batch */
+
+/* Batched isolated pressure solves (no counterpart in the reference as a batch: each snapshot is
+ * Pcg3D.solve's system, solver3d.ts:858-973, on a dense n^3 grid). Cells are PL_AIR / PL_FLUID /
+ * PL_SOLID, optionally with PL_POISSON_PIN on a FLUID cell: that cell's diagonal gets +1, the gauge fix
+ * of a liquid component without air contact (src/sim/pressure.ts:232-268; the caller also removes the
+ * component's rhs mean, as pl_poisson_generate does). FLUID cells on the grid border are not
+ * unknowns. Snapshots are stored back to back, x fastest. */
+#define PL_POISSON_PIN 4
+enum pl_poisson_method {
+  PL_POISSON_MIC0 = 0, /* the reference's MIC(0) (solver3d.ts:883-900, 955-973), level-scheduled */
+  PL_POISSON_MG = 1    /* one V-cycle of 3D geometric multigrid (src/sim/multigrid.ts in 3D, RBGS) */
+};
+/* Synthetic workload on the host: snapshots first .. first+count-1 of n^3 cells (n a power of two in
+ * [8, 512]): a solid cylinder wall (radius 60/128 n) and border, a liquid bottom slab (n/8) and 1-8
+ * liquid spheres (radius 6-24 cells at n = 128) from mulberry32 (src/sim/rng.ts:5-14) seeded 1000 +
+ * snapshot, AIR elsewhere; rhs = -div of a unit-variance Gaussian random face-velocity field
+ * (standard deviation 8 cells at n = 128) on the unknowns, with the gauge fix applied. threads <= 0:
+ * all hardware threads. cell: count * n^3 bytes, b: count * n^3 floats. */
+int pl_poisson_generate(int32_t n, int32_t first, int32_t count, uint8_t* cell, float* b, int32_t threads);
+/* The gauge fix on caller cells and rhs (host arrays, count snapshots of n^3): every 6-connected
+ * component of unknowns without an AIR neighbour gets its rhs mean removed and its first cell (index
+ * order) flagged PL_POISSON_PIN (fixEnclosedGauges, src/sim/pressure.ts:232-268). enclosed (may be
+ * NULL) receives the number of such components per snapshot. */
+int pl_poisson_gauge_fix(int32_t n, int32_t count, uint8_t* cell, float* b, int32_t* enclosed);
+typedef struct pl_poisson pl_poisson;
+/* Solver for `count` snapshots of n^3 cells with `method` and `precision` (PL_SOLVE_MIXED: FP32
+ * vectors, FP64 inner products, norms, solution and true-residual refinement; PL_SOLVE_F64: all
+ * FP64). Holds its device scratch until pl_poisson_destroy. */
+int pl_poisson_create(int32_t n, int32_t count, int32_t method, int32_t precision, pl_poisson** out);
+/* Solve every snapshot (device buffers: cell u8, b f32 and x f64, each count * n^3) on stream with
+ * the reference's stopping rule (max-norm residual <= max(tol * max|b|, 1e-14), at most max_iter
+ * iterations); writes per-snapshot iterations, final max-norm residual and converged flag to host
+ * arrays of count entries (any may be NULL). Synchronous. */
+int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double* x, double tol, int32_t max_iter,
+                     void* stream, int32_t* iterations, double* residual, int32_t* converged);
+/* Device bytes the solver holds. */
+size_t pl_poisson_device_bytes(const pl_poisson* h);
+void pl_poisson_destroy(pl_poisson* h);
+
 #ifdef __cplusplus
 }
 #endif

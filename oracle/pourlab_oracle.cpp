@@ -285,8 +285,9 @@ struct Pcg3D {
     list.assign(n, 0);
   }
 
+  // pin (may be null): cells whose diagonal gets +1, the gauge fix of src/sim/pressure.ts:265
   SolveResult solve(const uint8_t* cell, size_t ncell, const double* b, double* q, double tol,
-                    int maxIter) {  // solver3d.ts:858-937
+                    int maxIter, const uint8_t* pin = nullptr) {  // solver3d.ts:858-937
     const int nxy = nx * ny;
     std::fill(adiag.begin(), adiag.end(), 0);
     std::fill(ai.begin(), ai.end(), 0);
@@ -305,6 +306,7 @@ struct Pcg3D {
       double d = 0;
       for (int o : offs)
         if (cell[c + o] != SOLID) d++;
+      if (pin && pin[c]) d++;
       adiag[c] = d;
       ai[c] = cell[c + 1] == FLUID ? -1 : 0;
       aj[c] = cell[c + nx] == FLUID ? -1 : 0;
@@ -1247,6 +1249,29 @@ int plo_pcg_solve(const uint8_t* cell, const double* b, double* q, int32_t nx, i
                   double tol, int32_t max_iter, int32_t* converged, double* residual) {
   Pcg3D pcg(nx, ny, nz);
   SolveResult r = pcg.solve(cell, size_t(nx) * ny * nz, b, q, tol, max_iter);
+  if (converged) *converged = r.converged ? 1 : 0;
+  if (residual) *residual = r.residual;
+  return r.iterations;
+}
+
+// One snapshot of the Poisson batch: cells may carry PL_POISSON_PIN on FLUID cells (diagonal + 1);
+// FLUID cells on the grid border are not unknowns. FP64 Pcg3D.solve with MIC(0).
+int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,
+                      int32_t* converged, double* residual) {
+  const size_t nc = size_t(n) * n * n;
+  std::vector<uint8_t> base(nc), pin(nc);
+  for (int k = 0; k < n; k++)
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < n; i++) {
+        const size_t c = (size_t(k) * n + j) * n + i;
+        uint8_t t = cell[c] & 3;
+        const bool border = i == 0 || j == 0 || k == 0 || i == n - 1 || j == n - 1 || k == n - 1;
+        if (border && t == FLUID) t = AIR;  // a border FLUID cell is not an unknown: Dirichlet, like AIR
+        base[c] = t;
+        pin[c] = (t == FLUID && (cell[c] & 4)) ? 1 : 0;
+      }
+  Pcg3D pcg(n, n, n);
+  SolveResult r = pcg.solve(base.data(), nc, b, q, tol, max_iter, pin.data());
   if (converged) *converged = r.converged ? 1 : 0;
   if (residual) *residual = r.residual;
   return r.iterations;

@@ -46,6 +46,11 @@ int plo_get_field(const plo_sim* s, int32_t field, void* out, size_t count);
 int plo_pcg_solve(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny,
                   int32_t nz, double tol, int32_t max_iter, int32_t* converged, double* residual);
 
+/* One dense n^3 snapshot of the Poisson batch (cells may carry PL_POISSON_PIN: diagonal + 1, the gauge
+ * fix of src/sim/pressure.ts:232-268); FP64 MIC(0)-PCG as Pcg3D.solve. Returns the iterations. */
+int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,
+                      int32_t* converged, double* residual);
+
 /* Geometry (vessel3d.ts:46-103) for unit tests. */
 double plo_teapot_sdf(const pl_teapot* t, double x, double y, double z);
 int plo_in_cavity(const pl_teapot* t, double x, double y, double z);

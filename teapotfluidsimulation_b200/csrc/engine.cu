@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "cheb.h"
 #include "kernels.h"
+#include "poisson.h"
 #include "mg.h"
 #include "setup.h"
 
@@ -839,6 +840,75 @@ int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q,
                                   converged, residual, err, sizeof err);
   if (rc) return fail(rc, "%s", err);
   return PL_OK;
+}
+
+// ------------------------------------------------------------------ Poisson batch
+
+struct pl_poisson {
+  pl::PoissonImpl* impl;
+  int n, count, device;
+};
+
+int pl_poisson_generate(int32_t n, int32_t first, int32_t count, uint8_t* cell, float* b, int32_t threads) {
+  if (!cell || !b) return fail(PL_E_ARG, "pl_poisson_generate: null buffer");
+  if (n < 8 || n > 512 || (n & (n - 1)) || count < 1 || first < 0)
+    return fail(PL_E_ARG, "pl_poisson_generate: n must be a power of two in [8, 512] and count >= 1 (n=%d count=%d)",
+                n, count);
+  return pl::poisson_generate(n, first, count, cell, b, threads);
+}
+
+int pl_poisson_gauge_fix(int32_t n, int32_t count, uint8_t* cell, float* b, int32_t* enclosed) {
+  if (!cell || !b) return fail(PL_E_ARG, "pl_poisson_gauge_fix: null buffer");
+  if (n < 3 || count < 1) return fail(PL_E_ARG, "pl_poisson_gauge_fix: bad size n=%d count=%d", n, count);
+  const size_t nc = size_t(n) * n * n;
+  for (int s = 0; s < count; s++) {
+    const int e = pl::gauge_fix_one(n, cell + s * nc, b + s * nc);
+    if (enclosed) enclosed[s] = e;
+  }
+  return PL_OK;
+}
+
+int pl_poisson_create(int32_t n, int32_t count, int32_t method, int32_t precision, pl_poisson** out) {
+  if (!out) return fail(PL_E_ARG, "pl_poisson_create: null argument");
+  *out = nullptr;
+  if (n < 8 || n > 512 || (n & (n - 1)) || count < 1)
+    return fail(PL_E_ARG, "pl_poisson_create: n must be a power of two in [8, 512] and count >= 1 (n=%d count=%d)", n,
+                count);
+  if (method != PL_POISSON_MIC0 && method != PL_POISSON_MG)
+    return fail(PL_E_ARG, "pl_poisson_create: unknown method %d", method);
+  if (precision != PL_SOLVE_F64 && precision != PL_SOLVE_MIXED)
+    return fail(PL_E_ARG, "pl_poisson_create: unknown precision %d", precision);
+  if ((long long)n * n * n * count > (1ll << 31) - 1)
+    return fail(PL_E_ARG, "pl_poisson_create: %d snapshots of %d^3 cells exceed 2^31 cells", count, n);
+  char err[256] = "";
+  int rc = 0;
+  pl::PoissonImpl* impl = pl::poisson_create(n, count, method, precision, err, sizeof err, &rc);
+  if (!impl) return fail(rc ? rc : PL_E_CUDA, "%s", err);
+  pl_poisson* h = new pl_poisson{impl, n, count, 0};
+  cudaGetDevice(&h->device);
+  *out = h;
+  return PL_OK;
+}
+
+int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double* x, double tol, int32_t max_iter,
+                     void* stream, int32_t* iterations, double* residual, int32_t* converged) {
+  if (!h || !cell || !b || !x) return fail(PL_E_ARG, "pl_poisson_solve: null argument");
+  if (!(tol >= 0) || max_iter < 1) return fail(PL_E_ARG, "pl_poisson_solve: bad tolerance or iteration cap");
+  cudaSetDevice(h->device);
+  char err[256] = "";
+  int rc = pl::poisson_solve(h->impl, cell, b, x, tol, max_iter, (cudaStream_t)stream, iterations, residual, converged,
+                             err, sizeof err);
+  if (rc) return fail(rc, "%s", err);
+  return PL_OK;
+}
+
+size_t pl_poisson_device_bytes(const pl_poisson* h) { return h ? pl::poisson_bytes(h->impl) : 0; }
+
+void pl_poisson_destroy(pl_poisson* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  pl::poisson_destroy(h->impl);
+  delete h;
 }
 
 }  // extern "C"

@@ -1,0 +1,20 @@
+// Batched dense-grid pressure-Poisson solves (poisson.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pl {
+
+struct PoissonImpl;
+
+int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int threads);
+int gauge_fix_one(int n, uint8_t* cell, float* b);
+PoissonImpl* poisson_create(int n, int count, int method, int precision, char* err, size_t errlen, int* rc);
+int poisson_solve(PoissonImpl* h, const uint8_t* cell, const float* b, double* x, double tol, int max_iter,
+                  cudaStream_t st, int* iters, double* res, int* conv, char* err, size_t errlen);
+void poisson_destroy(PoissonImpl* h);
+size_t poisson_bytes(const PoissonImpl* h);
+
+}  // namespace pl

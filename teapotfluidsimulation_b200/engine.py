@@ -28,6 +28,7 @@ EXPORTED = [
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
     "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
+    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -91,6 +92,15 @@ def lib() -> C.CDLL:
     L.pl_stream.restype = C.c_void_p
     L.pl_enable_stage_timing.argtypes = [P, C.c_int32]
     L.pl_stage_times.argtypes = [P, fp]
+    L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
+    L.pl_poisson_gauge_fix.argtypes = [C.c_int32, C.c_int32, u8p, fp, C.POINTER(C.c_int32)]
+    L.pl_poisson_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(P)]
+    L.pl_poisson_solve.argtypes = [P, P, P, P, C.c_double, C.c_int32, P, C.POINTER(C.c_int32), dp,
+                                   C.POINTER(C.c_int32)]
+    L.pl_poisson_device_bytes.argtypes = [P]
+    L.pl_poisson_device_bytes.restype = C.c_size_t
+    L.pl_poisson_destroy.argtypes = [P]
+    L.pl_poisson_destroy.restype = None
     _lib = L
     return L
 
@@ -331,3 +341,62 @@ def pcg_solve_device_noalloc(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny:
                                              tol, max_iter, C.c_void_p(stream), C.byref(it), C.byref(conv),
                                              C.byref(res)))
     return it.value, bool(conv.value), res.value
+
+
+# ------------------------------------------------------------------ Poisson batch
+
+POISSON_MIC0 = 0
+POISSON_MG = 1
+POISSON_PIN = 4
+
+
+def poisson_generate(n: int, first: int, count: int, threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Synthetic snapshots first..first+count-1 (pl_poisson_generate): cells u8 and rhs f32, (count, n^3)."""
+    cell = np.zeros((count, n * n * n), np.uint8)
+    b = np.zeros((count, n * n * n), np.float32)
+    _check(lib().pl_poisson_generate(n, first, count, _ptr(cell, C.c_uint8), _ptr(b, C.c_float), threads))
+    return cell, b
+
+
+def poisson_gauge_fix(n: int, cell: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Gauge fix in place on (count, n^3) cells and rhs (pl_poisson_gauge_fix); returns enclosed counts."""
+    count = cell.shape[0]
+    assert cell.dtype == np.uint8 and b.dtype == np.float32 and cell.flags.c_contiguous and b.flags.c_contiguous
+    enc = np.zeros(count, np.int32)
+    _check(lib().pl_poisson_gauge_fix(n, count, _ptr(cell, C.c_uint8), _ptr(b, C.c_float), _ptr(enc, C.c_int32)))
+    return enc
+
+
+class PoissonBatch:
+    """Batched dense-grid pressure solver (pl_poisson_create / pl_poisson_solve) on device buffers."""
+
+    def __init__(self, n: int, count: int, method: int, precision: int):
+        self.n, self.count = n, count
+        h = C.c_void_p()
+        _check(lib().pl_poisson_create(n, count, method, precision, C.byref(h)))
+        self._h = h
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().pl_poisson_device_bytes(self._h))
+
+    def solve(self, cell_ptr: int, b_ptr: int, x_ptr: int, tol: float, max_iter: int, stream: int = 0):
+        """Solve on device pointers (cell u8, b f32, x f64); returns (iterations, residuals, converged)."""
+        it = np.zeros(self.count, np.int32)
+        res = np.zeros(self.count)
+        conv = np.zeros(self.count, np.int32)
+        _check(lib().pl_poisson_solve(self._h, C.c_void_p(cell_ptr), C.c_void_p(b_ptr), C.c_void_p(x_ptr), tol,
+                                      max_iter, C.c_void_p(stream), _ptr(it, C.c_int32), _ptr(res, C.c_double),
+                                      _ptr(conv, C.c_int32)))
+        return it, res, conv.astype(bool)
+
+    def destroy(self):
+        if self._h:
+            lib().pl_poisson_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
