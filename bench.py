@@ -12,6 +12,11 @@ clock around each call. The reference arm (--impl reference) times the CPU FP64 
 reference solver on the same workload (the reference itself is TypeScript and no JavaScript
 runtime exists on the box).
 
+A second, supplementary measurement (`poisson_batch` in the same line) solves the isolated
+pressure-Poisson batch (64 snapshots of 128^3 per GPU) with multigrid- and MIC(0)-preconditioned CG,
+each timed with CUDA events around the public pl_poisson_solve call on inputs resident in HBM (671 MB,
+larger than L2), beside the CPU FP64 oracle on a bounded sample.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: torchrun --nproc-per-node N bench.py --gpus N: every rank runs its own replica of the
 pour (the single pour does not shard); value is the sum over ranks, timed as the max over ranks.
@@ -26,6 +31,8 @@ import statistics
 import subprocess
 import sys
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -49,6 +56,9 @@ def parse():
                          "true-residual refinement; f64 = all FP64")
     ap.add_argument("--start", type=float, default=0.0, help="simulated seconds to advance before warm-up")
     ap.add_argument("--cpu-sample", type=int, default=60, help="substeps of the CPU baseline sample")
+    ap.add_argument("--poisson-n", type=int, default=128, help="grid of the isolated Poisson batch (0: skip it)")
+    ap.add_argument("--poisson-count", type=int, default=64, help="snapshots of the isolated Poisson batch per GPU")
+    ap.add_argument("--poisson-cpu-sample", type=int, default=4, help="snapshots the CPU oracle solves as its sample")
     return ap.parse_args()
 
 
@@ -198,6 +208,92 @@ def pcg_bytes_per_iteration(m: int, precond: str, precision: str) -> float:
     w = 4.0 if precision == "mixed" else 8.0
     deg = 12
     return m * ((4 * w + 16) + (4 * w + 16) + deg * (7 * w + 16) + 2 * w)
+
+
+def poisson_bytes_per_iteration(m: int) -> float:
+    """Algorithmic bytes of one MG-preconditioned PCG iteration over m unknowns (FP32 vectors, each array
+    once per pass): the PCG part (apply A 9, axpys 24, direction 12 = 45 B) plus one V-cycle, (4 smoothing
+    sweeps x 13 + residual 13 + transfer 8) x 8/7 (the coarse levels add 1/7) = 83.4 B."""
+    return m * (45.0 + (4 * 13 + 13 + 8) * 8.0 / 7.0)
+
+
+def mic0_bytes_per_iteration(m: int) -> float:
+    """The same for MIC(0): the PCG part plus the two triangular sweeps (26 B)."""
+    return m * (45.0 + 26.0)
+
+
+def run_poisson(args, world: int, rank: int) -> dict | None:
+    """The isolated pressure-Poisson batch: `count` snapshots of n^3 (rank r solves its own snapshots), MG- and
+    MIC(0)-preconditioned CG in FP32 vectors with FP64 inner products and refinement at the max-norm 1e-6
+    rule, each against an FP64 MG-PCG solve to 1e-12 of the same snapshots."""
+    if args.poisson_n <= 0:
+        return None
+    import torch
+
+    from teapotfluidsimulation_b200 import abi
+    from teapotfluidsimulation_b200 import engine as E
+
+    n, count = args.poisson_n, args.poisson_count
+    t0 = time.perf_counter()
+    cell, b = E.poisson_generate(n, rank * count, count)
+    gen_s = time.perf_counter() - t0
+    m_each = ((cell & 3) == abi.FLUID).sum(axis=1)  # unknowns per snapshot (border cells are SOLID)
+    dc = torch.from_numpy(cell).cuda()
+    db = torch.from_numpy(b).cuda()
+    del cell
+
+    def solve(method, precision, tol, reps):
+        x = torch.zeros((count, n ** 3), dtype=torch.float64, device="cuda")
+        pb = E.PoissonBatch(n, count, method, precision)
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            it, res, conv = pb.solve(dc.data_ptr(), db.data_ptr(), x.data_ptr(), tol, 4000)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = (ms, it, conv) if best is None or ms < best[0] else best
+        dev_bytes = pb.device_bytes
+        pb.destroy()
+        return x, best, dev_bytes
+
+    ref, (ref_ms, ref_it, ref_conv), _ = solve(E.POISSON_MG, abi.SOLVE_F64, 1e-12, 1)
+    refn = ref.abs().amax(dim=1).clamp_min(1e-300)
+    peaks, peak_kind = measured_peaks()
+    out = {"workload": f"{count} snapshots of {n}^3 per GPU (cylinder wall, slab, 1-8 mulberry32 spheres; "
+                       f"rhs = -div of a Gaussian random face field), seeds {1000 + rank * count}..",
+           "unknowns": int(m_each.sum()), "generate_s": gen_s, "tolerance": "max|r| <= 1e-6 max|b|",
+           "reference": {"method": "MG-PCG FP64 to 1e-12 (GPU; pinned to the CPU FP64 oracle in the tests)",
+                         "ms": ref_ms, "iterations_mean": float(ref_it.mean()), "converged": bool(ref_conv.all())}}
+    for name, method, reps, per_it in [("mg", E.POISSON_MG, 3, poisson_bytes_per_iteration),
+                                       ("mic0", E.POISSON_MIC0, 1, mic0_bytes_per_iteration)]:
+        x, (ms, it, conv), dev_bytes = solve(method, abi.SOLVE_MIXED, 1e-6, reps)
+        err = ((x - ref).abs().amax(dim=1) / refn).max().item()
+        del x
+        ms_max = allmax(ms, world)
+        work = float(sum(per_it(int(m)) * int(k) for m, k in zip(m_each, it)))
+        achieved = work / (ms / 1e3) / 1e9
+        out[name] = {"ms_per_batch": ms_max, "ms_per_snapshot": ms_max / count,
+                     "snapshots_per_s": allsum(count, world) / (ms_max / 1e3),
+                     "iterations_mean": float(it.mean()), "iterations_max": int(it.max()),
+                     "converged": bool(conv.all()), "max_rel_err_vs_fp64_1e-12": err, "device_gb": dev_bytes / 1e9,
+                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                                  "frac": achieved / peaks.get("hbm_gbs", 1.0), "peak_kind": peak_kind}}
+    out["mg_speedup_vs_mic0"] = out["mic0"]["ms_per_batch"] / out["mg"]["ms_per_batch"]
+    if rank == 0 and args.poisson_cpu_sample > 0:  # the CPU FP64 oracle (MIC(0)-PCG) on a bounded sample
+        from oracle import oracle as O
+
+        cs, bs = E.poisson_generate(n, 0, args.poisson_cpu_sample)
+        t0 = time.perf_counter()
+        for q in range(args.poisson_cpu_sample):
+            O.poisson_solve(cs[q], bs[q].astype(np.float64), n, tol=1e-6, max_iter=4000)
+        wall = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": args.poisson_cpu_sample / wall, "unit": "snapshots/s", "cores": 1,
+                               "kind": "port", "sample": f"{args.poisson_cpu_sample} snapshots of {n}^3, FP64 "
+                               f"MIC(0)-PCG (the C++ restatement of Pcg3D.solve) at the same 1e-6 rule"}
+    return out
 
 
 def run_cpu_baseline(args, substeps: int) -> dict:
@@ -363,6 +459,9 @@ def run_ours(args):
         line["clocks"] = clk
     if rank == 0 and world == 1:
         line["cpu_baseline"] = run_cpu_baseline(args, args.cpu_sample)
+    pois = run_poisson(args, world, rank)
+    if pois is not None:
+        line["poisson_batch"] = pois
     if rank == 0:
         print(json.dumps(line))
     e2e_sim.destroy()

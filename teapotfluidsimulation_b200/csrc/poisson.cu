@@ -312,7 +312,7 @@ __device__ __forceinline__ T wsum(const T* x, const T* w, int cells, int c, uint
 
 // Off-diagonal sum and diagonal of level (unit links and diagonal bytes when w is null).
 template <typename T>
-__device__ __forceinline__ void row(const T* x, const uint8_t* diag, const T* w, const T* dg, int cells, int c,
+__device__ __forceinline__ void row_sum(const T* x, const uint8_t* diag, const T* w, const T* dg, int cells, int c,
                                     uint8_t cd, int n, T& off, T& d) {
   if (w) {
     off = wsum(x, w, cells, c, cd, n);
@@ -326,62 +326,82 @@ __device__ __forceinline__ void row(const T* x, const uint8_t* diag, const T* w,
 // ---------------------------------------------------------------- multigrid kernels
 
 // One red-black half-sweep of colour `color` ((i + j + k) & 1) on a level: x = (b + sum of the
-// weighted unknown neighbours) / diagonal. first: the first half-sweep of a V-cycle from x = 0.
+// weighted unknown neighbours) / diagonal. first: the first half-sweep of a V-cycle from x = 0. One
+// thread per cell of the colour (128 of a tile's 256 cells), two tiles per CTA.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                    const T* w, const T* dg, int cells, T* x, const T* b,
                                                    int color, int first, const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    if (!tile_cell(G, list[ti], threadIdx.x, s, i, j, k, c)) continue;
-    if (st[s].done) continue;
-    const uint8_t cd = code[c];
-    if (!(cd & C_SELF) || ((i + j + k) & 1) != color) continue;
-    T off = T(0), d;
-    if (first) d = w ? dg[c] : T(diag[c]);
-    else row(x, diag, w, dg, cells, c, cd, G.n, off, d);
-    x[c] = (b[c] + off) / d;
-  }
+  const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
+  if (ti >= nact) return;
+  const int gt = list[ti];
+  const int s = gt >> G.lnt;
+  if (st[s].done) return;
+  const int u = threadIdx.x & 127;
+  const int hx = G.ltx - 1;  // log2 of the colour's cells per tile row
+  const int row = u >> hx;
+  const int lt = gt & ((1 << G.lnt) - 1);
+  const int ti_ = lt & (G.px - 1), tj = (lt >> G.lpx) & (G.py - 1), tk = lt >> (G.lpx + G.lpy);
+  const int j = (tj << G.lty) + (row & (G.ty - 1));
+  const int k = tk * G.tz + (row >> G.lty);
+  const int i = (ti_ << G.ltx) + 2 * (u & ((1 << hx) - 1)) + ((color + j + k) & 1);
+  const int c = (s << G.lnc) + (((k << G.ln) + j) << G.ln) + i;
+  const uint8_t cd = code[c];
+  if (!(cd & C_SELF)) return;
+  T off = T(0), d;
+  if (first) d = w ? dg[c] : T(diag[c]);
+  else row_sum(x, diag, w, dg, cells, c, cd, G.n, off, d);
+  x[c] = (b[c] + off) / d;
 }
 
-// Coarse right-hand side: the sum of the unknown children's residuals b - A x (P^T r).
+// Coarse right-hand side: the sum of the unknown children's residuals b - A x (P^T r). The last
+// pre-smoothing half-sweep updated the black cells from their red neighbours, so a black residual is
+// zero up to rounding and only the four red children ((dx + dy + dz) even) are summed. Two tiles per
+// CTA, two coarse cells per thread.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* listc, const uint8_t* codef,
                                                      const uint8_t* diagf, const T* wf, const T* dgf, int cellsf,
                                                      const T* xf, const T* bf, const uint8_t* codec, T* bc,
                                                      const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-  int s, i, j, k;
-  int c;
-  if (!tile_cell(Gc, listc[ti], threadIdx.x, s, i, j, k, c)) continue;
-  if (st[s].done) continue;
-  if (!(codec[c] & C_SELF)) continue;
+  const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
+  if (ti >= nact) return;
+  const int gt = listc[ti];
+  if (st[gt >> Gc.lnt].done) return;
   const int nf = Gf.n;
-  T acc = T(0);
 #pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const int dx = q & 1, dy = (q >> 1) & 1, dz = q >> 2;
-    const int cf = (s << Gf.lnc) + (((2 * k + dz) * nf + 2 * j + dy) * nf) + 2 * i + dx;
-    const uint8_t cd = codef[cf];
-    if (!(cd & C_SELF)) continue;
-    T off, d;
-    row(xf, diagf, wf, dgf, cellsf, cf, cd, nf, off, d);
-    acc += bf[cf] - (d * xf[cf] - off);
-  }
-  bc[c] = acc;
+  for (int q = 0; q < 2; q++) {
+    int s, i, j, k, c;
+    tile_cell(Gc, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
+    if (!(codec[c] & C_SELF)) continue;
+    const int base = (s << Gf.lnc) + ((2 * k) * nf + 2 * j) * nf + 2 * i;
+    const int kid[4] = {0, 1 + nf, 1 + nf * nf, nf + nf * nf};  // (0,0,0), (1,1,0), (1,0,1), (0,1,1)
+    T acc = T(0);
+#pragma unroll
+    for (int q2 = 0; q2 < 4; q2++) {
+      const int cf = base + kid[q2];
+      const uint8_t cd = codef[cf];
+      if (!(cd & C_SELF)) continue;
+      T off, d;
+      row_sum(xf, diagf, wf, dgf, cellsf, cf, cd, nf, off, d);
+      acc += bf[cf] - (d * xf[cf] - off);
+    }
+    bc[c] = acc;
   }
 }
 
 // x_fine += omega x_coarse(parent) where the parent is an unknown (multigrid.ts:150-156, over-relaxed).
+// Two tiles per CTA, two cells per thread.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* listf, const uint8_t* codef, T* xf,
                                                     const uint8_t* codec, const T* xc, const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    if (!tile_cell(Gf, listf[ti], threadIdx.x, s, i, j, k, c)) continue;
-    if (st[s].done) continue;
+  const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
+  if (ti >= nact) return;
+  const int gt = listf[ti];
+  if (st[gt >> Gf.lnt].done) return;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    int s, i, j, k, c;
+    tile_cell(Gf, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
     if (!(codef[c] & C_SELF)) continue;
     const int cc = (s << Gc.lnc) + (((k >> 1) * Gc.n + (j >> 1)) * Gc.n) + (i >> 1);
     if (codec[cc] & C_SELF) xf[c] += T(MG_OMEGA) * xc[cc];
@@ -518,65 +538,73 @@ __global__ void k_mic_bwd(TG G, const uint8_t* code, const T* pc, const T* qv, T
 
 // ---------------------------------------------------------------- PCG kernels
 
-__device__ __forceinline__ void block_sum_store(double v, double* out) {
+// Reduction of a half CTA (128 threads, one tile) into that tile's partial: sum or maximum. Every
+// thread of the CTA calls it; out is null for a half without a tile.
+__device__ __forceinline__ void half_store(double v, double* out, bool is_max) {
   __shared__ double sw[PT / 32];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    const double y = __shfl_xor_sync(0xffffffffu, v, o);
+    v = is_max ? fmax(v, y) : v + y;
+  }
   if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0;
-    for (int w = 0; w < PT / 32; w++) a += sw[w];
+  if ((threadIdx.x & 127) == 0 && out) {
+    const int w0 = (threadIdx.x >> 5);
+    double a = sw[w0];
+    for (int w = 1; w < 4; w++) a = is_max ? fmax(a, sw[w0 + w]) : a + sw[w0 + w];
     *out = a;
   }
-  __syncthreads();  // sw is reused by the next tile of the loop
+  __syncthreads();
 }
 
-__device__ __forceinline__ void block_max_atomic(double v, unsigned long long* out) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(v);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
-    b = ob > b ? ob : b;
-  }
-  if ((threadIdx.x & 31) == 0 && b) atomicMax(out, b);
-}
+// The PCG kernels run two tiles per CTA (a half CTA per tile, two cells per thread) and leave one
+// partial per tile.
+#define PCG_TILE_PROLOGUE                                   \
+  const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);       \
+  const bool has = ti < nact;                               \
+  const int gt = has ? list[ti] : 0;                        \
+  const int snap = gt >> G.lnt;                             \
+  const bool live = has && !st[snap].done;
 
 // r = b, x = 0, p = 0, |b| max per snapshot.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_init(TG G, const int* list, const uint8_t* code, const float* b, T* r,
-                                                 double* x, T* p, unsigned long long* bmax, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    double v = 0;
-    if (tile_cell(G, list[ti], threadIdx.x, s, i, j, k, c)) {
+                                                 double* x, T* p, double* part, const Snap* st, int nact) {
+  PCG_TILE_PROLOGUE
+  double v = 0;
+  if (has) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int s, i, j, k, c;
+      tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
       const bool u = code[c] & C_SELF;
       const double bv = u ? double(b[c]) : 0.0;
       r[c] = T(bv);
       x[c] = 0.0;
       p[c] = T(0);
-      v = fabs(bv);
-    } else {
-      s = list[ti] >> G.lnt;
+      v = fmax(v, fabs(bv));
     }
-    block_max_atomic(v, &bmax[s]);
   }
+  (void)live;
+  half_store(v, has ? &part[gt] : nullptr, true);
 }
 
 // Partial z.r per tile.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint8_t* code, const T* r, const T* z,
                                                double* part, const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    const int gt = list[ti];
-    double v = 0;
-    if (tile_cell(G, gt, threadIdx.x, s, i, j, k, c) && !st[s].done && (code[c] & C_SELF))
-      v = double(z[c]) * double(r[c]);
-    block_sum_store(v, &part[gt]);
+  PCG_TILE_PROLOGUE
+  double v = 0;
+  if (live) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int s, i, j, k, c;
+      tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
+      if (code[c] & C_SELF) v += double(z[c]) * double(r[c]);
+    }
   }
+  half_store(v, live ? &part[gt] : nullptr, false);
 }
 
 // p = z + beta p_old into p_new and A p_new (neighbours' new p formed on the fly from z and p_old, which
@@ -585,112 +613,118 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                 const T* z, const T* pold, T* pnew, T* ap, double* part,
                                                 const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-  int s, i, j, k;
-  int c;
-  const int gt = list[ti];
+  PCG_TILE_PROLOGUE
   double v = 0;
-  if (tile_cell(G, gt, threadIdx.x, s, i, j, k, c) && !st[s].done) {
-    const uint8_t cd = code[c];
-    if (cd & C_SELF) {
-      const T beta = T(st[s].beta);
-      const int n = G.n;
-      const int nxy = n * n;
-      auto pn = [&](int q) { return z[q] + beta * pold[q]; };
+  if (live) {
+    const T beta = T(st[snap].beta);
+    const int n = G.n, nxy = n * n;
+    auto pn = [&](int q) { return z[q] + beta * pold[q]; };
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int s, i, j, k, c;
+      tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
+      const uint8_t cd = code[c];
+      if (!(cd & C_SELF)) continue;
       const T pc = pn(c);
-      T a = (cd & 1) ? pn(c - 1) : T(0), b = (cd & 2) ? pn(c + 1) : T(0);
+      T a = (cd & 1) ? pn(c - 1) : T(0), b2 = (cd & 2) ? pn(c + 1) : T(0);
       T e = (cd & 4) ? pn(c - n) : T(0), f = (cd & 8) ? pn(c + n) : T(0);
       T g = (cd & 16) ? pn(c - nxy) : T(0), h = (cd & 32) ? pn(c + nxy) : T(0);
-      const T apv = T(diag[c]) * pc - (((a + b) + (e + f)) + (g + h));
+      const T apv = T(diag[c]) * pc - (((a + b2) + (e + f)) + (g + h));
       pnew[c] = pc;
       ap[c] = apv;
-      v = double(pc) * double(apv);
+      v += double(pc) * double(apv);
     }
   }
-  block_sum_store(v, &part[gt]);
-  }
+  half_store(v, live ? &part[gt] : nullptr, false);
 }
 
-// x += alpha p, r -= alpha Ap; max |r| per snapshot.
+// x += alpha p, r -= alpha Ap; max |r| per tile.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const uint8_t* code, double* x, const T* p,
-                                                   T* r, const T* ap, unsigned long long* rmax, const Snap* st,
-                                                   int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    double v = 0;
-    const int gt = list[ti];
-    s = gt >> G.lnt;
-    if (tile_cell(G, gt, threadIdx.x, s, i, j, k, c) && !st[s].done && (code[c] & C_SELF)) {
-      const double a = st[s].alpha;
+                                                   T* r, const T* ap, double* part, const Snap* st, int nact) {
+  PCG_TILE_PROLOGUE
+  double v = 0;
+  if (live) {
+    const double a = st[snap].alpha;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int s, i, j, k, c;
+      tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
+      if (!(code[c] & C_SELF)) continue;
       x[c] += a * double(p[c]);
       const T rv = r[c] - T(a) * ap[c];
       r[c] = rv;
-      v = fabs(double(rv));
+      v = fmax(v, fabs(double(rv)));
     }
-    block_max_atomic(v, &rmax[s]);
   }
+  half_store(v, live ? &part[gt] : nullptr, true);
 }
 
 // FP64 true residual b - A x of the snapshots in their check state; it replaces r.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
-                                                 const float* b, const double* x, T* r, unsigned long long* tmax,
+                                                 const float* b, const double* x, T* r, double* part,
                                                  const Snap* st, int nact) {
-  for (int ti = blockIdx.x; ti < nact; ti += gridDim.x) {
-    int s, i, j, k;
-    int c;
-    double v = 0;
-    const int gt = list[ti];
-    s = gt >> G.lnt;
-    if (tile_cell(G, gt, threadIdx.x, s, i, j, k, c) && !st[s].done && st[s].check && (code[c] & C_SELF)) {
+  PCG_TILE_PROLOGUE
+  const bool chk = live && st[snap].check;
+  double v = 0;
+  if (chk) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int s, i, j, k, c;
+      tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
       const uint8_t cd = code[c];
+      if (!(cd & C_SELF)) continue;
       const double rt = double(b[c]) - (double(diag[c]) * x[c] - nsum(x, c, cd, G.n));
       r[c] = T(rt);
-      v = fabs(rt);
+      v = fmax(v, fabs(rt));
     }
-    block_max_atomic(v, &tmax[s]);
   }
+  half_store(v, chk ? &part[gt] : nullptr, true);
 }
 
-// Per-snapshot scalar steps. phase 0: after init (bnorm, target); 1: after z.r (beta); 2: after
-// p.Ap (alpha, breakdown); 3: after the update (convergence, check); 4: after a true residual.
-__global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* part, long long ntile,
-                                                      unsigned long long* maxbits, Snap* st, double tol,
-                                                      int max_iter) {
+// Per-snapshot scalar steps from the per-tile partials (summed or maximised in tile order: inactive
+// tiles hold 0). phase 0: after init (max|b|: bnorm, target); 1: after z.r (beta); 2: after p.Ap
+// (alpha, breakdown); 3: after the update (max|r|: convergence, check); 4: after a true residual.
+__global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* part, long long ntile, Snap* st,
+                                                      double tol, int max_iter) {
   const int s = blockIdx.x;
   Snap& S = st[s];
   __shared__ double sw[RED_T / 32];
-  if (phase == 1 || phase == 2) {
-    if (S.done) return;
-    double a = 0;
-    for (long long t = threadIdx.x; t < ntile; t += RED_T) a += part[(long long)s * ntile + t];
+  if (phase != 0 && S.done) return;
+  if (phase == 4 && !S.check) return;
+  const bool is_max = phase == 0 || phase == 3 || phase == 4;
+  double a = 0;
+  for (long long t = threadIdx.x; t < ntile; t += RED_T) {
+    const double v = part[(long long)s * ntile + t];
+    a = is_max ? fmax(a, v) : a + v;
+  }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    double sum = 0;
-    for (int w = 0; w < RED_T / 32; w++) sum += sw[w];
-    if (phase == 1) {
-      S.rz_old = S.rz;
-      S.rz = sum;
-      S.beta = S.fresh ? 0.0 : sum / S.rz_old;
-      S.fresh = 0;
-    } else {
-      if (!(sum > 0)) {  // breakdown (solver3d.ts:913)
-        S.done = 1;
-        S.converged = S.res <= S.target ? 1 : 0;
-        return;
-      }
-      S.alpha = S.rz / sum;
-    }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_xor_sync(0xffffffffu, a, o);
+    a = is_max ? fmax(a, v) : a + v;
+  }
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double m = 0;
+  for (int w = 0; w < RED_T / 32; w++) m = is_max ? fmax(m, sw[w]) : m + sw[w];
+  if (phase == 1) {
+    S.rz_old = S.rz;
+    S.rz = m;
+    S.beta = S.fresh ? 0.0 : m / S.rz_old;
+    S.fresh = 0;
     return;
   }
-  if (threadIdx.x != 0) return;
-  const double m = __longlong_as_double((long long)maxbits[s]);
-  maxbits[s] = 0ull;
+  if (phase == 2) {
+    if (!(m > 0)) {  // breakdown (solver3d.ts:913)
+      S.done = 1;
+      S.converged = S.res <= S.target ? 1 : 0;
+      return;
+    }
+    S.alpha = S.rz / m;
+    return;
+  }
   if (phase == 0) {
     S.bnorm = m;
     S.target = fmax(tol * m, 1e-14);
@@ -704,7 +738,6 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
     if (S.done) S.converged = 1;
     return;
   }
-  if (S.done) return;
   if (phase == 3) {
     S.it++;
     S.res = m;
@@ -717,7 +750,6 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
     return;
   }
   // phase 4: true residual of a checked snapshot
-  if (!S.check) return;
   S.check = 0;
   if (m <= S.target || S.restarts >= 4) {
     S.res = m;
@@ -763,15 +795,11 @@ struct PoissonT : PoissonImpl {
   T *r = nullptr, *z = nullptr, *p = nullptr, *p1 = nullptr, *ap = nullptr, *pc = nullptr, *qv = nullptr;
   double* part = nullptr;
   Snap* st = nullptr;
-  unsigned long long* maxbits = nullptr;
   int* dcnt = nullptr;  // [PMAXLEV] active tile counters, [PMAXLEV] all-done flag
   int* chunk = nullptr;  // per-chunk counts / offsets of the list compaction
   int* pinned = nullptr;
   cudaGraphExec_t iter_graph = nullptr;
-  // CTAs of a tile kernel: one per active tile (measured faster than a grid-stride loop over the
-  // tiles with the GPU's resident CTA count), capped at max_blocks
-  int max_blocks = 1 << 30;
-  unsigned grid(int nact) const { return unsigned(std::max(1, std::min(nact, max_blocks))); }
+  static unsigned grid2(int nact) { return unsigned(std::max(1, (nact + 1) / 2)); }  // two tiles per CTA
 
   ~PoissonT() override {
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
@@ -813,7 +841,6 @@ struct PoissonT : PoissonImpl {
     const size_t i_qv = method == PL_POISSON_MIC0 ? add(C0 * sizeof(T)) : 0;
     const size_t i_part = add(size_t(count) * L[0].G.ntile * 8);
     const size_t i_st = add(size_t(count) * sizeof(Snap));
-    const size_t i_max = add(size_t(count) * 8);
     const size_t i_cnt = add(2 * PMAXLEV * 4);
     const size_t i_chunk = add(size_t((size_t(count) * L[0].G.ntile + CHUNK - 1) / CHUNK) * 4);
     size_t total = 0;
@@ -846,7 +873,6 @@ struct PoissonT : PoissonImpl {
     qv = method == PL_POISSON_MIC0 ? (T*)at[i_qv] : nullptr;
     part = (double*)at[i_part];
     st = (Snap*)at[i_st];
-    maxbits = (unsigned long long*)at[i_max];
     dcnt = (int*)at[i_cnt];
     chunk = (int*)at[i_chunk];
     e = cudaMemset(mem, 0, total);
@@ -905,8 +931,9 @@ struct PoissonT : PoissonImpl {
     auto B = [&](int l) -> const T* { return l == 0 ? r : L[l].b; };
     auto cells = [&](int l) { return (long long)count * L[l].G.nc; };
     auto smooth = [&](int l, int color, int first) {
-      k_mg_smooth<T><<<grid(L[l].nact), PT, 0, s0>>>(L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
-                                                     cells(l), X(l), B(l), color, first, st, L[l].nact);
+      k_mg_smooth<T><<<unsigned((L[l].nact + 1) / 2), PT, 0, s0>>>(L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w,
+                                                                   L[l].dg, cells(l), X(l), B(l), color, first, st,
+                                                                   L[l].nact);
     };
     const int top = nlev - 1;
     for (int l = 0; l < top; l++) {
@@ -916,7 +943,7 @@ struct PoissonT : PoissonImpl {
         smooth(l, 1, 0);
       }
       if (L[l + 1].nact)
-        k_mg_restrict<T><<<grid(L[l + 1].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
+        k_mg_restrict<T><<<grid2(L[l + 1].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
                                                              L[l].w, L[l].dg, cells(l), X(l), B(l), L[l + 1].code,
                                                              L[l + 1].b, st, L[l + 1].nact);
     }
@@ -938,7 +965,7 @@ struct PoissonT : PoissonImpl {
     for (int l = top - 1; l >= 0; l--) {
       if (L[l].nact == 0) continue;
       if (L[l + 1].nact)
-        k_mg_prolong<T><<<grid(L[l].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
+        k_mg_prolong<T><<<grid2(L[l].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
                                                         L[l + 1].code, L[l + 1].x, st, L[l].nact);
       for (int q = 0; q < MG_NU; q++) {
         smooth(l, 1, 0);
@@ -953,14 +980,14 @@ struct PoissonT : PoissonImpl {
     const TG& G = L[0].G;
     const int na = L[0].nact;
     precondition(s0);
-    k_pcg_rz<T><<<grid(na), PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, G.ntile, maxbits, st, tol, max_iter);
-    k_pcg_pap<T><<<grid(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, G.ntile, maxbits, st, tol, max_iter);
-    k_pcg_update<T><<<grid(na), PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, maxbits, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, G.ntile, maxbits, st, tol, max_iter);
-    k_pcg_true<T><<<grid(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, maxbits, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, G.ntile, maxbits, st, tol, max_iter);
+    k_pcg_rz<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, part, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, G.ntile, st, tol, max_iter);
+    k_pcg_pap<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, G.ntile, st, tol, max_iter);
+    k_pcg_update<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, part, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, G.ntile, st, tol, max_iter);
+    k_pcg_true<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, G.ntile, st, tol, max_iter);
   }
 
   int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t s0, int* iters,
@@ -972,11 +999,11 @@ struct PoissonT : PoissonImpl {
     }
     const TG& G = L[0].G;
     const int na = L[0].nact;
-    cudaMemsetAsync(maxbits, 0, size_t(count) * 8, s0);
+    cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);  // inactive tiles' partials stay 0
     cudaMemsetAsync(x, 0, size_t(count) * G.nc * 8, s0);
-    if (na > 0) k_pcg_init<T><<<grid(na), PT, 0, s0>>>(G, L[0].list, L[0].code, b, r, x, p, maxbits, na);
+    if (na > 0) k_pcg_init<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, b, r, x, p, part, st, na);
     cudaMemsetAsync(p1, 0, size_t(count) * G.nc * sizeof(T), s0);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, G.ntile, maxbits, st, tol, max_iter);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, G.ntile, st, tol, max_iter);
     if (na > 0) {
       // the iteration as a CUDA graph (one launch per iteration), checked for completion in batches
       if (iter_graph) {
