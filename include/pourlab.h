@@ -65,6 +65,16 @@ enum pl_preconditioner { PL_PRECOND_MIC0 = 0, PL_PRECOND_MG = 1, PL_PRECOND_CHEB
  * Krylov and smoother vectors in FP32 with FP64 inner products, an FP64 solution and FP64
  * iterative refinement of the true residual. */
 enum pl_solve_precision { PL_SOLVE_F64 = 0, PL_SOLVE_MIXED = 1 };
+/* Particle-grid transfer. FLIP is the reference's FLIP/PIC blend with flip_ratio
+ * (solver3d.ts:410-431, 607-624); APIC is the affine transfer of the 2D solver
+ * (src/sim/solver.ts:543-590, 944-990) in 3D: each parcel carries the gradient of every velocity
+ * component, P2G adds its affine term and G2P is the masked PIC sample plus the interpolant's
+ * gradient (flip_ratio unused). */
+enum pl_transfer { PL_TRANSFER_FLIP = 0, PL_TRANSFER_APIC = 1 };
+/* Simulated domain. HALF is the reference's half pot behind the symmetry plane z = h
+ * (solver3d.ts:9-10, 157, 756-760); FULL simulates both halves (the seeded half and its mirror image),
+ * with no symmetry plane. */
+enum pl_domain { PL_DOMAIN_HALF = 0, PL_DOMAIN_FULL = 1 };
 
 /* Teapot3DConfig (src/sim3d/vessel3d.ts:9-20). */
 typedef struct pl_teapot {
@@ -117,7 +127,9 @@ typedef struct pl_config {
   int32_t device;          /* CUDA device ordinal; -1 = the calling thread's current device */
   int32_t solve_cluster;   /* CTAs of the cluster solves (1-16; 0 = 16), see pl_autotune_solver */
   int32_t solve_threads;   /* threads per CTA of the cluster solves (32-1024; 0 = 512) */
-  int32_t reserved[3];
+  int32_t transfer;        /* enum pl_transfer */
+  int32_t domain;          /* enum pl_domain */
+  int32_t reserved;
 } pl_config;
 
 /* Diagnostics3D (src/sim3d/solver3d.ts:45-60). */
@@ -309,11 +321,17 @@ int pl_read_render_positions(pl_sim* sim, float* xyz6n);
 /* ------------------------------------------------------------------ state (parity harness) */
 
 /* Scalar state and parcel arrays in id order (FP64 SoA as in solver3d.ts:75-82). The engine
- * stores parcels in FP32, so pl_set_state rounds them. Any parcel pointer may be NULL on get. */
+ * stores parcels in FP32, so pl_set_state rounds them. Any parcel pointer may be NULL on get. With
+ * APIC, setting the parcels resets their affine vectors to zero. */
 int pl_get_state(pl_sim* sim, pl_sim_state* st);
 int pl_set_state(pl_sim* sim, const pl_sim_state* st, const double* x, const double* y,
                  const double* z, const double* vx, const double* vy, const double* vz,
                  const uint8_t* status);
+/* APIC state (no counterpart in the 3D reference; the 2D solver's cux/cuy/cvx/cvy,
+ * src/sim/solver.ts:91-94): per parcel id the gradients of u, v and w, 9 floats
+ * (du/dx, du/dy, du/dz, dv/dx, ..., dw/dz). PL_E_STATE unless the transfer is APIC. */
+int pl_get_affine(pl_sim* sim, float* c9);
+int pl_set_affine(pl_sim* sim, const float* c9);
 /* Copy one grid field of the last substep to host memory (enum pl_field); count is the number of
  * elements the caller's buffer holds. u8 fields are written as uint8_t, others as double. */
 int pl_get_field(pl_sim* sim, int32_t field, void* out, size_t count);

@@ -54,6 +54,8 @@ def lib() -> C.CDLL:
         L.plo_get_field.argtypes = [P, C.c_int32, P, C.c_size_t]
         L.plo_pcg_solve.argtypes = [u8p, dp, dp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
                                     C.POINTER(C.c_int32), dp]
+        L.plo_get_affine.argtypes = [P, dp]
+        L.plo_set_affine.argtypes = [P, dp]
         L.plo_poisson_solve.argtypes = [u8p, dp, dp, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32), dp]
         L.plo_teapot_sdf.argtypes = [C.POINTER(abi.Teapot), C.c_double, C.c_double, C.c_double]
         L.plo_teapot_sdf.restype = C.c_double
@@ -170,6 +172,20 @@ class OracleSim:
             stat = np.ascontiguousarray(parts["status"], dtype=np.uint8)
             ptrs = [_ptr(k, C.c_double) for k in keep] + [_ptr(stat, C.c_uint8)]
         lib().plo_set_state(self._h, C.byref(st) if st is not None else None, *ptrs)
+
+    def affine(self) -> np.ndarray:
+        """APIC affine state, (n, 3, 3): gradient of component a along axis b."""
+        out = np.zeros(self.n * 9)
+        lib().plo_get_affine(self._h, _ptr(out, C.c_double))
+        return out.reshape(self.n, 3, 3)
+
+    def set_affine(self, c):
+        """Set the APIC affine state from (n, 3, 3) or a (3, 3) matrix for every parcel."""
+        c = np.asarray(c, np.float64)
+        if c.shape == (3, 3):
+            c = np.broadcast_to(c, (self.n, 3, 3))
+        c = np.ascontiguousarray(c).reshape(-1)
+        lib().plo_set_affine(self._h, _ptr(c, C.c_double))
 
     def field(self, which: int) -> np.ndarray:
         n = self.nfaces if which in abi.FACE_FIELDS else self.nc

@@ -403,6 +403,7 @@ struct plo_sim {
   int n;
   double parcelVolume;
   std::vector<double> x, y, z, vx, vy, vz;
+  std::vector<double> aff[3][3];  // APIC: gradient of velocity component a along axis b, per parcel
   std::vector<uint8_t> origin, status;
   std::vector<float> y0;
   int bandCounts[3] = {0, 0, 0};
@@ -507,6 +508,8 @@ struct plo_sim {
     vx.assign(n, 0);
     vy.assign(n, 0);
     vz.assign(n, 0);
+    for (auto& row : aff)
+      for (auto& c : row) c.assign(n, 0);
     origin.assign(n, 0);
     status.assign(n, 0);
     y0.resize(n);
@@ -684,10 +687,25 @@ struct plo_sim {
       double o[3];
       int sz[3];
       dims(comp, o, sz);
+      const bool apic = cfg.transfer == PL_TRANSFER_APIC;
       for (int p = 0; p < n; p++) {
         if (status[p] != IN_POT) continue;
         size_t base = stencil(x[p], y[p], z[p], o[0], o[1], o[2], sz[0], sz[1], sz[2], st);
         double vp = vel[p];
+        if (apic) {  // affine field at each corner face (src/sim/solver.ts:553-587 in 3D)
+          const size_t sxy = size_t(sz[0]) * sz[1];
+          const double fi = double(base % sz[0]), fj = double((base / sz[0]) % sz[1]), fk = double(base / sxy);
+          const double cx = aff[comp][0][p], cy = aff[comp][1][p], cz = aff[comp][2][p];
+          const double d0x = (fi + o[0]) * h - x[p], d0y = (fj + o[1]) * h - y[p], d0z = (fk + o[2]) * h - z[p];
+          forEachCorner(base, sz[0], sz[1], [&](size_t idx, double wgt) {
+            const size_t rel = idx - base;
+            const int di = int(rel % sz[0]), dj = int((rel / sz[0]) % sz[1]), dk = int(rel / sxy);
+            const double a = vp + cx * (d0x + di * h) + cy * (d0y + dj * h) + cz * (d0z + dk * h);
+            f[idx] += wgt * a;
+            wt[idx] += wgt;
+          });
+          continue;
+        }
         forEachCorner(base, sz[0], sz[1], [&](size_t idx, double wgt) {
           f[idx] += wgt * vp;
           wt[idx] += wgt;
@@ -853,8 +871,42 @@ struct plo_sim {
     ex(w, wValid, nx, ny, nz + 1);
   }
 
+  // Gradient of component comp's trilinear interpolant at (px, py, pz) from the unmasked corners (the
+  // 3D form of src/sim/solver.ts:958-964).
+  void interpGradient(const std::vector<double>& field, int comp, double px, double py, double pz, double* g3) {
+    double o[3];
+    int sz[3];
+    dims(comp, o, sz);
+    size_t base = stencil(px, py, pz, o[0], o[1], o[2], sz[0], sz[1], sz[2], st);
+    const size_t sx = size_t(sz[0]), sxy = size_t(sz[0]) * sz[1];
+    double u[8];
+    for (int c = 0; c < 8; c++) u[c] = field[base + (c & 1) + ((c & 2) ? sx : 0) + ((c & 4) ? sxy : 0)];
+    const double fx = st[0], fy = st[1], fz = st[2];
+    g3[0] = ((1 - fy) * (1 - fz) * (u[1] - u[0]) + fy * (1 - fz) * (u[3] - u[2]) + (1 - fy) * fz * (u[5] - u[4]) +
+             fy * fz * (u[7] - u[6])) / h;
+    g3[1] = ((1 - fx) * (1 - fz) * (u[2] - u[0]) + fx * (1 - fz) * (u[3] - u[1]) + (1 - fx) * fz * (u[6] - u[4]) +
+             fx * fz * (u[7] - u[5])) / h;
+    g3[2] = ((1 - fx) * (1 - fy) * (u[4] - u[0]) + fx * (1 - fy) * (u[5] - u[1]) + (1 - fx) * fy * (u[6] - u[2]) +
+             fx * fy * (u[7] - u[3])) / h;
+  }
+
   void gridToParticles() {  // solver3d.ts:607-624
     double a = cfg.flip_ratio;
+    if (cfg.transfer == PL_TRANSFER_APIC) {  // src/sim/solver.ts:956-986 in 3D: PIC sample + gradient
+      const std::vector<double>* f[3] = {&u, &v, &w};
+      const std::vector<uint8_t>* va[3] = {&uValid, &vValid, &wValid};
+      std::vector<double>* vel[3] = {&vx, &vy, &vz};
+      for (int p = 0; p < n; p++) {
+        if (status[p] != IN_POT) continue;
+        for (int comp = 0; comp < 3; comp++) {
+          (*vel[comp])[p] = sample(*f[comp], comp, x[p], y[p], z[p], va[comp]);
+          double g3[3];
+          interpGradient(*f[comp], comp, x[p], y[p], z[p], g3);
+          for (int b = 0; b < 3; b++) aff[comp][b][p] = g3[b];
+        }
+      }
+      return;
+    }
     for (int p = 0; p < n; p++) {
       if (status[p] != IN_POT) continue;
       double px = x[p], py = y[p], pz = z[p];
@@ -1165,6 +1217,9 @@ int plo_set_state(plo_sim* s, const pl_sim_state* st, const double* x, const dou
   if (vx) std::memcpy(s->vx.data(), vx, n * 8);
   if (vy) std::memcpy(s->vy.data(), vy, n * 8);
   if (vz) std::memcpy(s->vz.data(), vz, n * 8);
+  if (x && y && z && status)  // new parcels: the APIC affine parts restart at zero (as in the engine)
+    for (auto& row : s->aff)
+      for (auto& c : row) std::fill(c.begin(), c.end(), 0.0);
   if (status) {
     std::memcpy(s->status.data(), status, n);
     for (int k = 0; k < 4; k++) s->counts[k] = 0;
@@ -1275,6 +1330,18 @@ int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n
   if (converged) *converged = r.converged ? 1 : 0;
   if (residual) *residual = r.residual;
   return r.iterations;
+}
+
+void plo_get_affine(const plo_sim* s, double* c9) {
+  for (int p = 0; p < s->n; p++)
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) c9[9 * p + 3 * a + b] = s->aff[a][b][p];
+}
+
+void plo_set_affine(plo_sim* s, const double* c9) {
+  for (int p = 0; p < s->n; p++)
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) s->aff[a][b][p] = c9[9 * p + 3 * a + b];
 }
 
 double plo_teapot_sdf(const pl_teapot* t, double x, double y, double z) {

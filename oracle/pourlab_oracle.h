@@ -46,6 +46,9 @@ int plo_get_field(const plo_sim* s, int32_t field, void* out, size_t count);
 int plo_pcg_solve(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny,
                   int32_t nz, double tol, int32_t max_iter, int32_t* converged, double* residual);
 
+/* APIC affine state per parcel id: 9 values (gradients of u, v, w). */
+void plo_get_affine(const plo_sim* s, double* c9);
+void plo_set_affine(plo_sim* s, const double* c9);
 /* One dense n^3 snapshot of the Poisson batch (cells may carry PL_POISSON_PIN: diagonal + 1, the gauge
  * fix of src/sim/pressure.ts:232-268); FP64 MIC(0)-PCG as Pcg3D.solve. Returns the iterations. */
 int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,

@@ -24,6 +24,8 @@ PHASES = ["wait", "tilt-in", "hold", "return", "rest", "done", "manual"]
 
 PRECOND_MIC0, PRECOND_MG, PRECOND_CHEB = 0, 1, 2
 SOLVE_F64, SOLVE_MIXED = 0, 1
+TRANSFER_FLIP, TRANSFER_APIC = 0, 1
+DOMAIN_HALF, DOMAIN_FULL = 0, 1
 
 FIELD_CELL = 0
 FIELD_VELOCITY = 1
@@ -89,7 +91,9 @@ class Config(C.Structure):
         ("device", C.c_int32),
         ("solve_cluster", C.c_int32),
         ("solve_threads", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("transfer", C.c_int32),
+        ("domain", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

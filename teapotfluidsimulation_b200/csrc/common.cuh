@@ -61,6 +61,9 @@ struct Geo {
   int solve_threads;
   int ntx, nty;  // column tiles along x and y
   int tiled;     // the cluster solver orders its cells by column tile (ntx * nty * nz <= TILE_PLANES_MAX)
+  int apic;      // affine particle-grid transfer (PL_TRANSFER_APIC)
+  int full;      // both halves of the pot, no symmetry plane (PL_DOMAIN_FULL)
+  double zoff;   // world z of the pot-local plane z = 0 (h for the half domain)
   double parcel_volume;
   double R;  // Math.hypot(nx, ny) * h  (solver3d.ts:275)
   // teapot
@@ -135,7 +138,7 @@ PL_HD void to_local(const Geo& g, double c, double s, double wx, double wy, doub
   double ry = DSUB(wy, g.pwy);
   out[0] = DADD(DADD(DMUL(c, rx), DMUL(s, ry)), g.pivx);
   out[1] = DADD(DADD(DMUL(-s, rx), DMUL(c, ry)), g.pivy);
-  out[2] = DSUB(wz, g.h);
+  out[2] = DSUB(wz, g.zoff);
 }
 
 PL_HD void to_world(const Geo& g, double c, double s, double lx, double ly, double lz, double* out) {
@@ -143,7 +146,7 @@ PL_HD void to_world(const Geo& g, double c, double s, double lx, double ly, doub
   double ry = DSUB(ly, g.pivy);
   out[0] = DADD(DSUB(DMUL(c, rx), DMUL(s, ry)), g.pwx);
   out[1] = DADD(DADD(DMUL(s, rx), DMUL(c, ry)), g.pwy);
-  out[2] = DADD(lz, g.h);
+  out[2] = DADD(lz, g.zoff);
 }
 
 PL_HD double dmax(double a, double b) { return a > b ? a : b; }
@@ -244,6 +247,8 @@ __device__ __forceinline__ uint8_t cell_at(const Geo& g, const uint8_t* cell, in
 struct DevPtrs {
   // parcels
   float4 *pos_home, *vel_home, *pos_sorted, *vel_sorted, *frac_sorted, *frac_tmp;
+  // APIC: per parcel the gradients of u, v and w (xyz of three float4, aff[comp * n + p]), in both orders
+  float4 *aff_home, *aff_sorted;
   int *key, *rank;
   int2* placed;  // (id, home slot) in bin order before the in-bin sort
   // bins and cells

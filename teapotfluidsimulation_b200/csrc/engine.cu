@@ -285,6 +285,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       size_t(g.ntx) * g.nty * g.nz * 8,                // column-tile masks
       C * 6 * 4, C * 4,                                // tile-order neighbours, permutation
       C, C * 3 * 27 * 8, C * 27 * 4,                   // occupancy, node partials (velocity, density)
+      g.apic ? N * 48 : 16, g.apic ? N * 48 : 16,      // APIC affine vectors (home, sorted)
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -341,6 +342,8 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.occ = (uint8_t*)take();
   P.m_vel = (float2*)take();
   P.m_den = (float*)take();
+  P.aff_home = (float4*)take();
+  P.aff_sorted = (float4*)take();
   mg_configure();
   cheb_configure();
   int nn = g.n;
@@ -654,6 +657,63 @@ int pl_read_particles(pl_sim* s, float* pos4, float* vel4, uint32_t* status) {
   return PL_OK;
 }
 
+// Slot of every parcel id in the home layout.
+static int home_slots(pl_sim* s, std::vector<int>& slot) {
+  const int n = s->g.n;
+  std::vector<float4> hp(n);
+  CK(cudaMemcpyAsync(hp.data(), s->P.pos_home, size_t(n) * 16, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  slot.assign(n, -1);
+  for (int i = 0; i < n; i++) {
+    int id;
+    std::memcpy(&id, &hp[i].w, 4);
+    if (id < 0 || id >= n) return fail(PL_E_STATE, "parcel layout corrupt (id %d at slot %d)", id, i);
+    slot[id] = i;
+  }
+  return PL_OK;
+}
+
+int pl_get_affine(pl_sim* s, float* c9) {
+  if (!s || !c9) return fail(PL_E_ARG, "pl_get_affine: null argument");
+  if (!s->g.apic) return fail(PL_E_STATE, "pl_get_affine: the simulation does not use APIC");
+  cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
+  std::vector<int> slot;
+  if ((rc = home_slots(s, slot))) return rc;
+  const int n = s->g.n;
+  std::vector<float4> a(size_t(3) * n);
+  CK(cudaMemcpyAsync(a.data(), s->P.aff_home, size_t(n) * 48, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  for (int id = 0; id < n; id++)
+    for (int comp = 0; comp < 3; comp++) {
+      const float4 v = a[size_t(comp) * n + slot[id]];
+      c9[9 * id + 3 * comp] = v.x;
+      c9[9 * id + 3 * comp + 1] = v.y;
+      c9[9 * id + 3 * comp + 2] = v.z;
+    }
+  return PL_OK;
+}
+
+int pl_set_affine(pl_sim* s, const float* c9) {
+  if (!s || !c9) return fail(PL_E_ARG, "pl_set_affine: null argument");
+  if (!s->g.apic) return fail(PL_E_STATE, "pl_set_affine: the simulation does not use APIC");
+  cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
+  std::vector<int> slot;
+  if ((rc = home_slots(s, slot))) return rc;
+  const int n = s->g.n;
+  std::vector<float4> a(size_t(3) * n);
+  for (int id = 0; id < n; id++)
+    for (int comp = 0; comp < 3; comp++)
+      a[size_t(comp) * n + slot[id]] =
+          make_float4(c9[9 * id + 3 * comp], c9[9 * id + 3 * comp + 1], c9[9 * id + 3 * comp + 2], 0.f);
+  CK(cudaMemcpyAsync(s->P.aff_home, a.data(), size_t(n) * 48, cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return PL_OK;
+}
+
 int pl_read_particles_f64(pl_sim* s, double* x, double* y, double* z, double* vx, double* vy, double* vz,
                           uint8_t* status) {
   if (!s) return fail(PL_E_ARG, "pl_read_particles_f64: null handle");
@@ -727,6 +787,7 @@ int pl_set_state(pl_sim* s, const pl_sim_state* st, const double* x, const doubl
   if (x && y && z && status) {
     int rc = upload_parcels(s, x, y, z, vx, vy, vz, status);
     if (rc) return rc;
+    if (s->g.apic) CK(cudaMemsetAsync(s->P.aff_home, 0, size_t(n) * 48, s->st));  // affine parts restart at 0
     for (int k = 0; k < 4; k++) h.counts[k] = 0;
     for (int k = 0; k < 3; k++) h.by_origin[k] = 0;
     double m = 0;

@@ -295,6 +295,9 @@ __global__ void k_bin_permute(Geo g, DevPtrs P) {
   P.pos_sorted[dst] = P.pos_home[e.y];
   P.vel_sorted[dst] = P.vel_home[e.y];
   P.frac_sorted[dst] = P.frac_tmp[e.y];
+  if (g.apic)
+#pragma unroll
+    for (int a = 0; a < 3; a++) P.aff_sorted[a * g.n + dst] = P.aff_home[a * g.n + e.y];
 }
 
 // ---------------------------------------------------------------- particle-to-grid
@@ -326,13 +329,15 @@ __device__ __forceinline__ void axis_w3(float f, bool half, double w[3]) {
 // velocity component (COMP 0..2, particlesToGrid, solver3d.ts:410-431), or of w alone (COMP 3, the
 // density of densityCorrection, solver3d.ts:633-642). A node's full sum is then a fixed-order sum of
 // at most 18 (velocity) or 27 (density) partials, so the face and density gathers issue independent
-// loads instead of walking every parcel of the neighbourhood.
-template <int COMP>
+// loads instead of walking every parcel of the neighbourhood. With APIC the velocity carried to a node
+// is the parcel's affine field there, v + c . (x_node - x_p) (src/sim/solver.ts:553-587 in 3D).
+template <int COMP, bool APIC>
 __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int c, int p0, int p1) {
   constexpr bool hx = COMP != 0, hy = COMP != 1, hz = COMP != 2;
   double sw[27], swv[27];
 #pragma unroll
   for (int q = 0; q < 27; q++) sw[q] = swv[q] = 0.0;
+  const int ci = c % g.nx, cj = (c / g.nx) % g.ny, ck = c / (g.nx * g.ny);
   for (int p = p0; p < p1; p++) {
     const float4 fr = P.frac_sorted[p];
     double v = 0.0;
@@ -341,6 +346,18 @@ __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int
     axis_w3(fr.x, hx, wx);
     axis_w3(fr.y, hy, wy);
     axis_w3(fr.z, hz, wz);
+    // APIC: the affine field at the node offsets, v + cx dx + cy dy + cz dz per axis term
+    double ax[3] = {0, 0, 0}, ay[3] = {0, 0, 0}, az[3] = {0, 0, 0};
+    if (APIC && COMP < 3) {
+      const float4 ps = P.pos_sorted[p];
+      const float4 ca = P.aff_sorted[COMP * g.n + p];
+#pragma unroll
+      for (int o = 0; o < 3; o++) {  // node at offset o - 1 from the cell on each axis
+        ax[o] = (double)ca.x * ((ci + o - 1 + (hx ? 0.5 : 0.0)) * g.h - (double)ps.x);
+        ay[o] = (double)ca.y * ((cj + o - 1 + (hy ? 0.5 : 0.0)) * g.h - (double)ps.y);
+        az[o] = (double)ca.z * ((ck + o - 1 + (hz ? 0.5 : 0.0)) * g.h - (double)ps.z);
+      }
+    }
 #pragma unroll
     for (int ox = 0; ox < 3; ox++) {
       if (!hx && ox == 0) continue;
@@ -353,7 +370,7 @@ __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int
           const int q = ox * 9 + oy * 3 + oz;
           const double w = wx[ox] * wy[oy] * wz[oz];
           sw[q] += w;
-          if (COMP < 3) swv[q] += w * v;
+          if (COMP < 3) swv[q] += w * (APIC ? v + ax[ox] + ay[oy] + az[oz] : v);
         }
       }
     }
@@ -377,11 +394,20 @@ __global__ void k_p2g_cells(Geo g, DevPtrs P) {
   if (c >= g.nc) return;
   const int p0 = P.start[c], p1 = P.start[c + 1];
   if (p0 == p1) return;
-  switch (blockIdx.y) {
-    case 0: cell_moments<0>(g, P, c, p0, p1); break;
-    case 1: cell_moments<1>(g, P, c, p0, p1); break;
-    case 2: cell_moments<2>(g, P, c, p0, p1); break;
-    default: cell_moments<3>(g, P, c, p0, p1); break;
+  if (g.apic) {
+    switch (blockIdx.y) {
+      case 0: cell_moments<0, true>(g, P, c, p0, p1); break;
+      case 1: cell_moments<1, true>(g, P, c, p0, p1); break;
+      case 2: cell_moments<2, true>(g, P, c, p0, p1); break;
+      default: cell_moments<3, true>(g, P, c, p0, p1); break;
+    }
+  } else {
+    switch (blockIdx.y) {
+      case 0: cell_moments<0, false>(g, P, c, p0, p1); break;
+      case 1: cell_moments<1, false>(g, P, c, p0, p1); break;
+      case 2: cell_moments<2, false>(g, P, c, p0, p1); break;
+      default: cell_moments<3, false>(g, P, c, p0, p1); break;
+    }
   }
 }
 
@@ -735,6 +761,25 @@ __device__ __forceinline__ double sample_valid(const Geo& g, const float* field,
   return ws > 1e-9 ? acc / ws : all;
 }
 
+// Gradient of the trilinear interpolant of component comp at (x, y, z), unmasked corners (the 3D form
+// of C = sum_i u_i grad w_ip, src/sim/solver.ts:958-964): per axis the corner differences along it,
+// weighted by the other two axes' weights, over h.
+__device__ __forceinline__ float4 interp_gradient(const Geo& g, const float* field, int comp, double x, double y,
+                                                  double z) {
+  Sten s = face_stencil(g, comp, x, y, z);
+  double u[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) u[c] = (double)field[corner(s, c)];
+  const double fx = s.fx, fy = s.fy, fz = s.fz;
+  const double gx = ((1 - fy) * (1 - fz) * (u[1] - u[0]) + fy * (1 - fz) * (u[3] - u[2]) +
+                     (1 - fy) * fz * (u[5] - u[4]) + fy * fz * (u[7] - u[6])) / g.h;
+  const double gy = ((1 - fx) * (1 - fz) * (u[2] - u[0]) + fx * (1 - fz) * (u[3] - u[1]) +
+                     (1 - fx) * fz * (u[6] - u[4]) + fx * fz * (u[7] - u[5])) / g.h;
+  const double gz = ((1 - fx) * (1 - fy) * (u[4] - u[0]) + fx * (1 - fy) * (u[5] - u[1]) +
+                     (1 - fx) * fy * (u[6] - u[2]) + fx * fy * (u[7] - u[3])) / g.h;
+  return make_float4((float)gx, (float)gy, (float)gz, 0.f);
+}
+
 // Correction velocity uc at face corners: the gradient of the correction potential evaluated on
 // the fly (applyGradient into zeroed uc,vc,wc: solver3d.ts:629-631, 674).
 __device__ __forceinline__ double sample_corr(const Geo& g, const DevPtrs& P, int comp, double x, double y,
@@ -783,8 +828,17 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
   }
   const double x0 = pos.x, y0 = pos.y, z0 = pos.z;
   double vx = vel.x, vy = vel.y, vz = vel.z;
-  // gridToParticles (solver3d.ts:607-624): FLIP/PIC blend with valid-masked samples
-  {
+  // gridToParticles (solver3d.ts:607-624): FLIP/PIC blend with valid-masked samples; APIC: the masked
+  // PIC sample and the gradient of each component's interpolant (src/sim/solver.ts:956-986 in 3D)
+  if (g.apic) {
+    const float* U = P.u;
+    const uint8_t* V = P.valid;
+    vx = sample_valid(g, U, V, 0, x0, y0, z0);
+    vy = sample_valid(g, U, V, 1, x0, y0, z0);
+    vz = sample_valid(g, U, V, 2, x0, y0, z0);
+#pragma unroll
+    for (int a = 0; a < 3; a++) P.aff_home[a * g.n + p] = interp_gradient(g, U, a, x0, y0, z0);
+  } else {
     const float* U = P.u;
     const float* UP = P.uprev;
     const uint8_t* V = P.valid;

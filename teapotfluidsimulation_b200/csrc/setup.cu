@@ -49,6 +49,7 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
   g = Geo{};
   const double h = cfg.h;
   g.h = h;
+  g.zoff = h;  // world z of the pot's symmetry plane (toLocal, solver3d.ts:232-240)
   // buildTeapot3D (vessel3d.ts:46-59)
   double a = (t.spout_angle_deg * PI) / 180;
   g.radius = t.radius;
@@ -172,6 +173,15 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
   g.ntx = (g.nx + TILE_W - 1) / TILE_W;
   g.nty = (g.ny + TILE_W - 1) / TILE_W;
   g.tiled = g.ntx * g.nty * g.nz <= TILE_PLANES_MAX ? 1 : 0;
+  if (cfg.transfer != PL_TRANSFER_FLIP && cfg.transfer != PL_TRANSFER_APIC) {
+    snprintf(err, errlen, "pl_create: unknown transfer %d", cfg.transfer);
+    return PL_E_ARG;
+  }
+  if (cfg.domain != PL_DOMAIN_HALF && cfg.domain != PL_DOMAIN_FULL) {
+    snprintf(err, errlen, "pl_create: unknown domain %d", cfg.domain);
+    return PL_E_ARG;
+  }
+  g.apic = cfg.transfer == PL_TRANSFER_APIC ? 1 : 0;
   g.solve_cluster = cfg.solve_cluster > 0 ? cfg.solve_cluster : 16;
   g.solve_threads = cfg.solve_threads > 0 ? cfg.solve_threads : 512;
   if (g.solve_cluster > 16 || g.solve_threads < 32 || g.solve_threads > 1024 || g.solve_threads % 32) {

@@ -28,7 +28,7 @@ EXPORTED = [
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
     "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
-    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
+    "pl_get_affine", "pl_set_affine", "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -92,6 +92,8 @@ def lib() -> C.CDLL:
     L.pl_stream.restype = C.c_void_p
     L.pl_enable_stage_timing.argtypes = [P, C.c_int32]
     L.pl_stage_times.argtypes = [P, fp]
+    L.pl_get_affine.argtypes = [P, fp]
+    L.pl_set_affine.argtypes = [P, fp]
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
     L.pl_poisson_gauge_fix.argtypes = [C.c_int32, C.c_int32, u8p, fp, C.POINTER(C.c_int32)]
     L.pl_poisson_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(P)]
@@ -305,6 +307,20 @@ class Simulation3D:
             stat = np.ascontiguousarray(parts["status"], dtype=np.uint8)
             ptrs = [_ptr(k, C.c_double) for k in keep] + [_ptr(stat, C.c_uint8)]
         _check(lib().pl_set_state(self._h, C.byref(st) if st is not None else None, *ptrs))
+
+    def affine(self) -> np.ndarray:
+        """APIC affine state (pl_get_affine), (n, 3, 3): gradient of component a along axis b."""
+        out = np.zeros(self.n * 9, np.float32)
+        _check(lib().pl_get_affine(self.handle, _ptr(out, C.c_float)))
+        return out.reshape(self.n, 3, 3)
+
+    def set_affine(self, c):
+        """pl_set_affine from (n, 3, 3) or one (3, 3) matrix for every parcel."""
+        c = np.asarray(c, np.float32)
+        if c.shape == (3, 3):
+            c = np.broadcast_to(c, (self.n, 3, 3))
+        c = np.ascontiguousarray(c).reshape(-1)
+        _check(lib().pl_set_affine(self.handle, _ptr(c, C.c_float)))
 
     def field(self, which: int) -> np.ndarray:
         n = self.nfaces if which in abi.FACE_FIELDS else self.nc
