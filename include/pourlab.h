@@ -314,8 +314,9 @@ int pl_read_particles_f64(pl_sim* sim, double* x, double* y, double* z, double* 
 /* Simulation3D.origin (solver3d.ts:81): origin layer 0/1/2 per parcel id. */
 int pl_read_origin(const pl_sim* sim, uint8_t* origin);
 /* readRenderPositions() (src/gpu3d/solver.ts:443-475; kernel src/gpu3d/shaders.ts:786-799):
- * packed xyz of the simulated half then its mirror image, 6*n floats, written by a device kernel
- * into a device buffer and copied to xyz6n. */
+ * packed xyz of the simulated half then its mirror image, 6*n floats (PL_DOMAIN_FULL: the xyz of
+ * the n simulated parcels, 3*n floats), written by a device kernel into a device buffer and copied
+ * to xyz6n. */
 int pl_read_render_positions(pl_sim* sim, float* xyz6n);
 
 /* ------------------------------------------------------------------ state (parity harness) */

@@ -402,6 +402,8 @@ struct plo_sim {
   double pivotWorld[2];
   int n;
   double parcelVolume;
+  double zoff = 0;       // world z of the pot-local plane z = 0 (h for the half domain)
+  double volFactor = 2;  // the half stands for the pot (2); both halves simulated (1)
   std::vector<double> x, y, z, vx, vy, vz;
   std::vector<double> aff[3][3];  // APIC: gradient of velocity component a along axis b, per parcel
   std::vector<uint8_t> origin, status;
@@ -427,6 +429,7 @@ struct plo_sim {
   // solver3d.ts:116-228
   void construct() {
     h = cfg.h;
+    zoff = h;  // the half domain's plane; the full domain moves it after seeding
     const pl_teapot& t = cfg.teapot;
     fillHeight = cfg.initial_volume / (PI * t.radius * t.radius);
     const double pts[6][2] = {
@@ -459,28 +462,6 @@ struct plo_sim {
     nx = int(std::ceil((x1 - x0 + 2 * m) / h));
     ny = int(std::ceil((y1 - y0v + 2 * m) / h));
     nz = int(std::ceil((t.radius + t.wall + 2 * h) / h)) + 1;
-    size_t nc = size_t(nx) * ny * nz;
-    cell.assign(nc, 0);
-    size_t nu = size_t(nx + 1) * ny * nz, nv = size_t(nx) * (ny + 1) * nz, nw = size_t(nx) * ny * (nz + 1);
-    u.assign(nu, 0);
-    uPrev.assign(nu, 0);
-    uw.assign(nu, 0);
-    uValid.assign(nu, 0);
-    uc.assign(nu, 0);
-    v.assign(nv, 0);
-    vPrev.assign(nv, 0);
-    vw.assign(nv, 0);
-    vValid.assign(nv, 0);
-    vc.assign(nv, 0);
-    w.assign(nw, 0);
-    wPrev.assign(nw, 0);
-    ww.assign(nw, 0);
-    wValid.assign(nw, 0);
-    wc.assign(nw, 0);
-    rhs.assign(nc, 0);
-    q.assign(nc, 0);
-    density.assign(nc, 0);
-    pcg = new Pcg3D(nx, ny, nz);
 
     Rng rng(cfg.seed);
     double s = h / 2;
@@ -532,6 +513,53 @@ struct plo_sim {
       origin[order[r]] = uint8_t(k);
       bandCounts[k]++;
     }
+    volFactor = 2;
+    if (cfg.domain == PL_DOMAIN_FULL) {
+      // Full domain (no counterpart in the reference): both halves, the symmetry plane a cell face at
+      // world z = zoff, every seeded parcel plus its mirror image (ids n..2n-1, same origin layer).
+      const int nzHalf = nz;
+      nz = 2 * nzHalf - 2;
+      zoff = (nzHalf - 1) * h;
+      const int nh = n;
+      n = 2 * nh;
+      x.resize(n), y.resize(n), z.resize(n), vx.assign(n, 0), vy.assign(n, 0), vz.assign(n, 0);
+      origin.resize(n), status.assign(n, 0), y0.resize(n);
+      for (auto& row : aff)
+        for (auto& c : row) c.assign(n, 0);
+      for (int p = 0; p < nh; p++) {
+        const double lz = z[p] - h;
+        z[p] = lz + zoff;
+        x[nh + p] = x[p];
+        y[nh + p] = y[p];
+        z[nh + p] = -lz + zoff;
+        origin[nh + p] = origin[p];
+        y0[nh + p] = y0[p];
+      }
+      for (int k = 0; k < 3; k++) bandCounts[k] *= 2;
+      volFactor = 1;
+    }
+    size_t nc = size_t(nx) * ny * nz;
+    cell.assign(nc, 0);
+    size_t nu = size_t(nx + 1) * ny * nz, nv = size_t(nx) * (ny + 1) * nz, nw = size_t(nx) * ny * (nz + 1);
+    u.assign(nu, 0);
+    uPrev.assign(nu, 0);
+    uw.assign(nu, 0);
+    uValid.assign(nu, 0);
+    uc.assign(nu, 0);
+    v.assign(nv, 0);
+    vPrev.assign(nv, 0);
+    vw.assign(nv, 0);
+    vValid.assign(nv, 0);
+    vc.assign(nv, 0);
+    w.assign(nw, 0);
+    wPrev.assign(nw, 0);
+    ww.assign(nw, 0);
+    wValid.assign(nw, 0);
+    wc.assign(nw, 0);
+    rhs.assign(nc, 0);
+    q.assign(nc, 0);
+    density.assign(nc, 0);
+    pcg = new Pcg3D(nx, ny, nz);
     counts[0] = n;
     counts[1] = counts[2] = counts[3] = 0;
   }
@@ -544,7 +572,7 @@ struct plo_sim {
     double ry = wy - pivotWorld[1];
     out[0] = c * rx + s * ry + cfg.pivot[0];
     out[1] = -s * rx + c * ry + cfg.pivot[1];
-    out[2] = wz - h;
+    out[2] = wz - zoff;
   }
   void toWorldAt(double ph, double lx, double ly, double lz, double* out) const {
     double c = std::cos(ph), s = std::sin(ph);
@@ -552,7 +580,7 @@ struct plo_sim {
     double ry = ly - cfg.pivot[1];
     out[0] = c * rx - s * ry + pivotWorld[0];
     out[1] = s * rx + c * ry + pivotWorld[1];
-    out[2] = lz + h;
+    out[2] = lz + zoff;
   }
 
   bool finished() const { return time >= cfg.duration - 1e-9; }  // solver3d.ts:264-266
@@ -575,7 +603,7 @@ struct plo_sim {
   }
 
   void step(double dt) {  // solver3d.ts:288-309
-    double discharged = counts[DISCHARGED] * parcelVolume * 2;
+    double discharged = counts[DISCHARGED] * parcelVolume * volFactor;
     double tilt1 = controller.advance(time + dt, dt, discharged);
     double phi1 = -tilt1;
     omega = (phi1 - phi) / dt;
@@ -1038,7 +1066,7 @@ struct plo_sim {
           vz[p] -= rn * nwz;
         }
       }
-      if (z1 < h) {
+      if (cfg.domain != PL_DOMAIN_FULL && z1 < h) {  // symmetry plane (half domain)
         z1 = 2 * h - z1;
         vz[p] = std::fabs(vz[p]);
       }
@@ -1064,13 +1092,14 @@ struct plo_sim {
       double r = hypot2(loc1[0], loc1[2]);
       bool insideBody = r < pc.radius + 2 * pc.wall && loc1[1] > -2 * pc.wall;
       bool nearSpout = loc1[0] > 0 && loc1[0] < pot.tipX + 0.03;
-      bool atEdge = x1 <= lo || y1 <= lo || x1 >= hiX || y1 >= hiY || z1 >= hiZ;
+      bool atEdge = x1 <= lo || y1 <= lo || x1 >= hiX || y1 >= hiY || z1 >= hiZ ||
+                    (cfg.domain == PL_DOMAIN_FULL && z1 <= lo);
       if ((!insideBody && !nearSpout) || atEdge) setStatus(p, SPILLED);
     }
   }
 
   void diagnostics(pl_diagnostics* d) const {  // solver3d.ts:796-814
-    double vml = parcelVolume * 2 * 1e6;
+    double vml = parcelVolume * volFactor * 1e6;
     d->time = time;
     d->steps = steps;
     d->angle_deg = controller.angle / DEG;

@@ -64,6 +64,7 @@ struct Geo {
   int apic;      // affine particle-grid transfer (PL_TRANSFER_APIC)
   int full;      // both halves of the pot, no symmetry plane (PL_DOMAIN_FULL)
   double zoff;   // world z of the pot-local plane z = 0 (h for the half domain)
+  double vol_factor;  // parcels' volume scale in the accounting: 2 (the half stands for the pot), 1 (full)
   double parcel_volume;
   double R;  // Math.hypot(nx, ny) * h  (solver3d.ts:275)
   // teapot

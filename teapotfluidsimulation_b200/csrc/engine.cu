@@ -594,7 +594,7 @@ int pl_get_diagnostics(pl_sim* s, pl_diagnostics* d) {  // solver3d.ts:796-814
   int rc = settle(s);
   if (rc) return rc;
   const SimScalars& h = s->hs;
-  const double v = s->g.parcel_volume * 2 * 1e6;
+  const double v = s->g.parcel_volume * s->g.vol_factor * 1e6;
   std::memset(d, 0, sizeof *d);
   d->time = h.time;
   d->steps = h.steps;
@@ -747,7 +747,8 @@ int pl_read_render_positions(pl_sim* s, float* xyz6n) {
   cudaSetDevice(s->device);
   launch_render(s->g, s->P, s->st);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(xyz6n, s->P.render, size_t(s->g.n) * 6 * 4, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaMemcpyAsync(xyz6n, s->P.render, size_t(s->g.n) * (s->g.full ? 3 : 6) * 4, cudaMemcpyDeviceToHost,
+                     s->st));
   CK(cudaStreamSynchronize(s->st));
   return PL_OK;
 }

@@ -51,7 +51,7 @@ __global__ void k_controller(Geo g, DevPtrs P) {
   sc->force_step = 0;
   sc->forced_dt = 0;
   // step(dt) (solver3d.ts:288-292)
-  double discharged = sc->counts[DISCHARGED] * g.parcel_volume * 2;
+  double discharged = sc->counts[DISCHARGED] * g.parcel_volume * g.vol_factor;
   double tilt1 = ctl_advance(sc->motion, sc->ctl, sc->time + dt, dt, discharged);
   double phi1 = -tilt1;
   sc->omega = (phi1 - sc->phi) / dt;
@@ -899,7 +899,7 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
       vz -= rn * nwz;
     }
   }
-  if (z1 < g.h) {  // symmetry plane
+  if (!g.full && z1 < g.h) {  // symmetry plane (half domain only)
     z1 = 2 * g.h - z1;
     vz = fabs(vz);
   }
@@ -935,7 +935,7 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
     bool near_spout = loc1[0] > 0 && loc1[0] < g.tipx + 0.03;
     double lo = g.h * 1.01;
     bool at_edge = x1 <= lo || y1 <= lo || x1 >= (g.nx - 1) * g.h || y1 >= (g.ny - 1) * g.h ||
-                   z1 >= (g.nz - 1) * g.h;
+                   z1 >= (g.nz - 1) * g.h || (g.full && z1 <= lo);
     if ((!inside_body && !near_spout) || at_edge) new_st = SPILLED;
   }
   if (new_st != IN_POT) {
@@ -980,10 +980,11 @@ __global__ void k_render(Geo g, DevPtrs P) {
   int id = __float_as_int(p.w);
   float x = p.x, y = p.y, z = p.z;
   if (y < 0.0005f) y = -100.0f;
-  int m = id + g.n;
   P.render[3 * id] = x;
   P.render[3 * id + 1] = y;
   P.render[3 * id + 2] = z;
+  if (g.full) return;  // both halves are simulated: no mirror image
+  int m = id + g.n;
   P.render[3 * m] = x;
   P.render[3 * m + 1] = y;
   P.render[3 * m + 2] = (float)(2.0 * g.h) - z;

@@ -98,7 +98,13 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
   }
   g.nx = int(fnx);
   g.ny = int(fny);
-  g.nz = int(fnz);
+  g.nz = int(fnz);  // the half domain's z extent; the full domain is resized after seeding
+  const int nz_half = g.nz;
+  const bool full = cfg.domain == PL_DOMAIN_FULL;
+  if (full && 2.0 * fnx * fny * fnz > 6.0e7) {
+    snprintf(err, errlen, "pl_create: full-domain grid %gx%gx%g out of range", fnx, fny, 2 * fnz - 2);
+    return PL_E_ARG;
+  }
   g.nc = g.nx * g.ny * g.nz;
   g.nu = (g.nx + 1) * g.ny * g.nz;
   g.nv = g.nx * (g.ny + 1) * g.nz;
@@ -159,6 +165,40 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
     out->origin[order[r]] = uint8_t(k);
     out->band_counts[k]++;
   }
+  g.vol_factor = 2;
+  if (full) {
+    // Full domain: both halves. The z grid mirrors the interior cells about the pot's symmetry plane,
+    // which becomes a cell face at world z = zoff; every seeded parcel gets its mirror image (ids
+    // n..2n-1, same origin layer), so the seeded half is the reference's, and the pot holds both.
+    g.nz = 2 * nz_half - 2;
+    g.zoff = (nz_half - 1) * h;
+    out->x.resize(2 * size_t(n));
+    out->y.resize(2 * size_t(n));
+    out->z.resize(2 * size_t(n));
+    out->origin.resize(2 * size_t(n));
+    for (int p = 0; p < n; p++) {
+      const double lz = out->z[p] - h;  // pot-local z of the seeded parcel (half-domain frame)
+      out->z[p] = lz + g.zoff;
+      out->x[n + p] = out->x[p];
+      out->y[n + p] = out->y[p];
+      out->z[n + p] = -lz + g.zoff;
+      out->origin[n + p] = out->origin[p];
+    }
+    for (int k = 0; k < 3; k++) out->band_counts[k] *= 2;
+    g.n = 2 * n;
+    g.vol_factor = 1;
+    g.nc = g.nx * g.ny * g.nz;
+    g.nu = (g.nx + 1) * g.ny * g.nz;
+    g.nv = g.nx * (g.ny + 1) * g.nz;
+    g.nw = g.nx * g.ny * (g.nz + 1);
+    g.nf = g.nu + g.nv + g.nw;
+    g.nbins = g.nc + REMOVED_BINS;
+    if (g.nbins > SCAN_MAX_BINS) {
+      snprintf(err, errlen, "pl_create: %d cells exceed the bin scan capacity", g.nc);
+      return PL_E_ARG;
+    }
+  }
+  g.full = full ? 1 : 0;
   // physics
   g.gravity = cfg.gravity;
   g.flip = cfg.flip_ratio;

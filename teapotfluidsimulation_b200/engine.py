@@ -289,8 +289,9 @@ class Simulation3D:
         return o
 
     def read_render_positions(self) -> np.ndarray:
-        """readRenderPositions() (src/gpu3d/solver.ts:443-475): xyz of the half, then the mirror."""
-        out = np.zeros(6 * self.n, np.float32)
+        """readRenderPositions() (src/gpu3d/solver.ts:443-475): xyz of the half, then the mirror (full
+        domain: the xyz of every parcel)."""
+        out = np.zeros((3 if self.cfg.domain == abi.DOMAIN_FULL else 6) * self.n, np.float32)
         _check(lib().pl_read_render_positions(self._h, _ptr(out, C.c_float)))
         return out
 
