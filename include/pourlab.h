@@ -404,6 +404,31 @@ int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double*
 size_t pl_poisson_device_bytes(const pl_poisson* h);
 void pl_poisson_destroy(pl_poisson* h);
 
+/* ------------------------------------------------------------------ learned preconditioner */
+
+/* A 3-level 3D convolutional U-Net (16/32/64 channels, 3^3 kernels, BF16 weights and activations,
+ * FP32 accumulation) that maps a residual r to an approximate correction z ~ A^-1 r on the liquid
+ * cells of a box (no counterpart in the reference). Inputs: [r / max|r|, liquid mask, air mask];
+ * output scaled by max|r| and zero off the liquid. Boxes are nx x ny x nz cells (multiples of 4), count
+ * of them back to back, x fastest; cell u8 (PL_AIR / PL_FLUID / PL_SOLID), r, z, e f32, all device
+ * buffers. Parameters are FP32 masters (per layer W[27][cin][cout] then the biases), trained by Adam
+ * on the relative squared error sum_liquid (z - e)^2 / sum_liquid e^2, averaged over the boxes. */
+typedef struct pl_unet pl_unet;
+int pl_unet_create(uint32_t seed, pl_unet** out);
+int32_t pl_unet_num_params(const pl_unet* u);
+int pl_unet_get_params(pl_unet* u, float* host);
+int pl_unet_set_params(pl_unet* u, const float* host); /* also resets the Adam moments */
+int pl_unet_apply(pl_unet* u, const uint8_t* cell, const float* r, float* z, int32_t nx, int32_t ny, int32_t nz,
+                  int32_t count, void* stream);
+/* One Adam step (learning rate lr) on the boxes' (r, e) pairs; the loss before the step to *loss. */
+int pl_unet_train_step(pl_unet* u, const uint8_t* cell, const float* r, const float* e, int32_t nx, int32_t ny,
+                       int32_t nz, int32_t count, float lr, float* loss, void* stream);
+/* The loss and its gradient with respect to every parameter (host array of pl_unet_num_params floats)
+ * without a step. Synchronous. */
+int pl_unet_gradient(pl_unet* u, const uint8_t* cell, const float* r, const float* e, int32_t nx, int32_t ny,
+                     int32_t nz, int32_t count, float* loss, float* grad, void* stream);
+void pl_unet_destroy(pl_unet* u);
+
 #ifdef __cplusplus
 }
 #endif

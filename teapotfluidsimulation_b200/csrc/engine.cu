@@ -17,6 +17,7 @@
 #include "cheb.h"
 #include "kernels.h"
 #include "poisson.h"
+#include "unet.h"
 #include "mg.h"
 #include "setup.h"
 
@@ -971,6 +972,78 @@ void pl_poisson_destroy(pl_poisson* h) {
   cudaSetDevice(h->device);
   pl::poisson_destroy(h->impl);
   delete h;
+}
+
+// ------------------------------------------------------------------ learned preconditioner
+
+struct pl_unet {
+  pl::UNetImpl* impl;
+  int device;
+};
+
+int pl_unet_create(uint32_t seed, pl_unet** out) {
+  if (!out) return fail(PL_E_ARG, "pl_unet_create: null argument");
+  *out = nullptr;
+  char err[256] = "";
+  int rc = 0;
+  pl::UNetImpl* impl = pl::unet_create(seed, err, sizeof err, &rc);
+  if (!impl) return fail(rc ? rc : PL_E_CUDA, "%s", err);
+  pl_unet* u = new pl_unet{impl, 0};
+  cudaGetDevice(&u->device);
+  *out = u;
+  return PL_OK;
+}
+
+int32_t pl_unet_num_params(const pl_unet* u) { return u ? pl::unet_nparams(u->impl) : 0; }
+
+int pl_unet_get_params(pl_unet* u, float* host) {
+  if (!u || !host) return fail(PL_E_ARG, "pl_unet_get_params: null argument");
+  cudaSetDevice(u->device);
+  int rc = pl::unet_get_params(u->impl, host);
+  return rc ? fail(rc, "pl_unet_get_params: %s", cudaGetErrorString(cudaGetLastError())) : PL_OK;
+}
+
+int pl_unet_set_params(pl_unet* u, const float* host) {
+  if (!u || !host) return fail(PL_E_ARG, "pl_unet_set_params: null argument");
+  cudaSetDevice(u->device);
+  int rc = pl::unet_set_params(u->impl, host);
+  return rc ? fail(rc, "pl_unet_set_params: %s", cudaGetErrorString(cudaGetLastError())) : PL_OK;
+}
+
+int pl_unet_apply(pl_unet* u, const uint8_t* cell, const float* r, float* z, int32_t nx, int32_t ny, int32_t nz,
+                  int32_t count, void* stream) {
+  if (!u || !cell || !r || !z) return fail(PL_E_ARG, "pl_unet_apply: null argument");
+  cudaSetDevice(u->device);
+  char err[256] = "";
+  int rc = pl::unet_apply(u->impl, cell, r, z, nx, ny, nz, count, (cudaStream_t)stream, err, sizeof err);
+  return rc ? fail(rc, "%s", err) : PL_OK;
+}
+
+int pl_unet_train_step(pl_unet* u, const uint8_t* cell, const float* r, const float* e, int32_t nx, int32_t ny,
+                       int32_t nz, int32_t count, float lr, float* loss, void* stream) {
+  if (!u || !cell || !r || !e || !loss) return fail(PL_E_ARG, "pl_unet_train_step: null argument");
+  cudaSetDevice(u->device);
+  char err[256] = "";
+  int rc = pl::unet_gradient(u->impl, cell, r, e, nx, ny, nz, count, lr, 1, loss, nullptr, (cudaStream_t)stream, err,
+                             sizeof err);
+  return rc ? fail(rc, "%s", err) : PL_OK;
+}
+
+int pl_unet_gradient(pl_unet* u, const uint8_t* cell, const float* r, const float* e, int32_t nx, int32_t ny,
+                     int32_t nz, int32_t count, float* loss, float* grad, void* stream) {
+  if (!u || !cell || !r || !e || !loss || !grad) return fail(PL_E_ARG, "pl_unet_gradient: null argument");
+  cudaSetDevice(u->device);
+  char err[256] = "";
+  int rc = pl::unet_gradient(u->impl, cell, r, e, nx, ny, nz, count, 0.f, 0, loss, grad, (cudaStream_t)stream, err,
+                             sizeof err);
+  return rc ? fail(rc, "%s", err) : PL_OK;
+}
+
+void pl_unet_destroy(pl_unet* u) {
+  if (!u) return;
+  cudaSetDevice(u->device);
+  pl::unet_destroy(u->impl);
+  delete u;
 }
 
 }  // extern "C"

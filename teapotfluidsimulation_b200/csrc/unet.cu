@@ -1,0 +1,769 @@
+// Learned preconditioner: a 3-level 3D convolutional U-Net (16/32/64 channels, 3^3 kernels, BF16
+// weights and activations, FP32 accumulation), trained and applied with this file's own kernels.
+//
+// The network maps a residual field on a box of X x Y x Z cells (multiples of 4) to an approximate
+// correction: input channels [r / s, liquid mask, air mask] with s = max |r| over the liquid cells,
+// output z = s * net(...)[0] on the liquid cells (0 elsewhere). Layers (channels padded to multiples
+// of 16; every conv 3^3, zero padding, bias, ReLU except the last):
+//   enc1: 16->16, 16->16 (s1)        level 1 (X, Y, Z)
+//   enc2: pool, 16->32, 32->32 (s2)  level 2 (X/2, ...), 2x2x2 average pooling
+//   enc3: pool, 32->64, 64->64       level 3 (X/4, ...)
+//   dec2: up, [up | s2] 96->32, 32->32     nearest-neighbour upsampling, channel concatenation
+//   dec1: up, [up | s1] 48->16, 16->16
+//   out : 16->16 (channel 0 used)
+//
+// Kernels (NDHWC activations, x fastest among the cells, channels innermost):
+//  - k_conv: implicit GEMM out[v][n] = bias[n] + sum_t sum_k in[v + off_t][k] G[t][n][k] on the tensor
+//    cores (mma.sync m16n8k16, BF16 in, FP32 accumulate), one warp per 16 cells x all output
+//    channels; A and B fragments are loaded straight from the NDHWC tensor and the [tap][n][k] weights.
+//    The same kernel computes the data gradient with G[t][n][k] = W[26 - t][n][k] (flipped taps).
+//  - k_wgrad: weight gradient dW[t][ci][co] = sum_v in[v + off_t][ci] d[v][co] on the tensor cores:
+//    a CTA stages a chunk of cells of both operands transposed in shared memory ([channel][cell]) and
+//    accumulates the Cin x Cout tile; per-chunk partials are summed in a fixed order (deterministic).
+//  - pooling, upsampling, concatenation, ReLU masks, the loss and Adam are elementwise kernels.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "unet.h"
+
+namespace pl {
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int NLAYER = 11;
+constexpr int WG_CHUNK = 2048;  // cells per weight-gradient CTA
+constexpr int WG_KC = 32;       // cells per shared-memory stage of the weight gradient
+
+struct LayerSpec {
+  int cin, cout;
+};
+constexpr LayerSpec SPEC[NLAYER] = {{16, 16}, {16, 16}, {16, 32}, {32, 32}, {32, 64}, {64, 64},
+                                    {96, 32}, {32, 32}, {48, 16}, {16, 16}, {16, 16}};
+
+__device__ __forceinline__ uint32_t ld32(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ void mma16816(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct Box {
+  int X, Y, Z, count;
+  __host__ __device__ int cells() const { return X * Y * Z; }
+  __host__ __device__ int total() const { return X * Y * Z * count; }
+};
+
+// Cell index of the neighbour of cell v (global over the batch) at tap t (offsets -1..1, tap = dz*9 +
+// dy*3 + dx), or -1 outside the box.
+__device__ __forceinline__ int tap_cell(const Box& B, int v, int t) {
+  const int per = B.cells();
+  const int s = v / per;
+  const int c = v - s * per;
+  const int x = c % B.X, y = (c / B.X) % B.Y, z = c / (B.X * B.Y);
+  const int xx = x + t % 3 - 1, yy = y + (t / 3) % 3 - 1, zz = z + t / 9 - 1;
+  if (xx < 0 || yy < 0 || zz < 0 || xx >= B.X || yy >= B.Y || zz >= B.Z) return -1;
+  return s * per + (zz * B.Y + yy) * B.X + xx;
+}
+
+// Implicit-GEMM 3^3 convolution on NDHWC BF16 tensors. One warp per 16 output cells, all NOUT output
+// channels (NOUT = 16, 32 or 64: NOUT / 8 tiles of 8); K = 27 taps x CIN input channels in steps of 16.
+// out_f32 (optional): FP32 result; out_bf (optional): BF16 result after the optional ReLU; mask
+// (optional): the result is multiplied by (mask > 0) (the ReLU of the layer that produced the input
+// whose gradient this is).
+template <int NOUT>
+__global__ void __launch_bounds__(128) k_conv(Box B, const bf16* __restrict__ in, int cin, const bf16* __restrict__ G,
+                                              const float* __restrict__ bias, int relu, const bf16* __restrict__ mask,
+                                              bf16* out_bf, float* out_f32) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
+  const int v0 = warp * 16;
+  const int total = B.total();
+  if (v0 >= total) return;
+  constexpr int NT = NOUT / 8;
+  float acc[NT][4];
+#pragma unroll
+  for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const int va = v0 + g, vb = v0 + g + 8;  // the two rows this lane feeds
+  for (int t = 0; t < 27; t++) {
+    const int na = va < total ? tap_cell(B, va, t) : -1;
+    const int nb = vb < total ? tap_cell(B, vb, t) : -1;
+    const bf16* pa = na >= 0 ? in + (size_t)na * cin : nullptr;
+    const bf16* pb = nb >= 0 ? in + (size_t)nb * cin : nullptr;
+    const bf16* gt = G + (size_t)t * NOUT * cin;
+    for (int k0 = 0; k0 < cin; k0 += 16) {
+      const uint32_t a0 = pa ? ld32(pa + k0 + 2 * tg) : 0u;
+      const uint32_t a1 = pb ? ld32(pb + k0 + 2 * tg) : 0u;
+      const uint32_t a2 = pa ? ld32(pa + k0 + 2 * tg + 8) : 0u;
+      const uint32_t a3 = pb ? ld32(pb + k0 + 2 * tg + 8) : 0u;
+#pragma unroll
+      for (int j = 0; j < NT; j++) {
+        const bf16* gb = gt + (size_t)(j * 8 + g) * cin + k0 + 2 * tg;
+        mma16816(acc[j], a0, a1, a2, a3, ld32(gb), ld32(gb + 8));
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NT; j++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int v = h ? vb : va;
+      if (v >= total) continue;
+      const int n = j * 8 + 2 * tg;
+      float r0 = acc[j][2 * h], r1 = acc[j][2 * h + 1];
+      if (bias) {
+        r0 += bias[n];
+        r1 += bias[n + 1];
+      }
+      if (relu) {
+        r0 = fmaxf(r0, 0.f);
+        r1 = fmaxf(r1, 0.f);
+      }
+      if (mask) {
+        const bf16* m = mask + (size_t)v * NOUT + n;
+        if (!(__bfloat162float(m[0]) > 0.f)) r0 = 0.f;
+        if (!(__bfloat162float(m[1]) > 0.f)) r1 = 0.f;
+      }
+      if (out_f32) {
+        out_f32[(size_t)v * NOUT + n] = r0;
+        out_f32[(size_t)v * NOUT + n + 1] = r1;
+      }
+      if (out_bf) {
+        __nv_bfloat162 p;
+        p.x = __float2bfloat16(r0);
+        p.y = __float2bfloat16(r1);
+        *reinterpret_cast<__nv_bfloat162*>(out_bf + (size_t)v * NOUT + n) = p;
+      }
+    }
+  }
+}
+
+// Weight gradient of one tap t = blockIdx.y: part[chunk][t][ci][co] = sum over the CTA's cells v of
+// in[v + off_t][ci] d[v][co]. Shared memory holds WG_KC cells of both operands transposed
+// ([channel][cell]), so the A fragment (row = ci, k = cell) and the B fragment (k = cell, col = co) read
+// consecutive cells. 4 warps; warp w owns the 16-row blocks w, w + 4 of Cin (CIN <= 96: 6 blocks).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_wgrad(Box B, const bf16* __restrict__ in, const bf16* __restrict__ d,
+                                               float* part) {
+  constexpr int MB = CIN / 16, NT = COUT / 8;
+  constexpr int LD = WG_KC + 8;  // padded row (cells) in shared memory
+  __shared__ __align__(16) bf16 sa[CIN * LD];
+  __shared__ __align__(16) bf16 sb[COUT * LD];
+  const int t = blockIdx.y;
+  const int total = B.total();
+  const int c0 = blockIdx.x * WG_CHUNK;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
+  float acc[2][NT][4];
+#pragma unroll
+  for (int m = 0; m < 2; m++)
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[m][j][0] = acc[m][j][1] = acc[m][j][2] = acc[m][j][3] = 0.f;
+  for (int base = c0; base < min(c0 + WG_CHUNK, total); base += WG_KC) {
+    __syncthreads();
+    // stage: thread -> (cell, channel pair)
+    for (int e = threadIdx.x; e < WG_KC * (CIN / 2); e += blockDim.x) {
+      const int k = e / (CIN / 2), cp = (e % (CIN / 2)) * 2;
+      const int v = base + k;
+      const int nv = v < total ? tap_cell(B, v, t) : -1;
+      bf16 x0 = __float2bfloat16(0.f), x1 = x0;
+      if (nv >= 0) {
+        x0 = in[(size_t)nv * CIN + cp];
+        x1 = in[(size_t)nv * CIN + cp + 1];
+      }
+      sa[cp * LD + k] = x0;
+      sa[(cp + 1) * LD + k] = x1;
+    }
+    for (int e = threadIdx.x; e < WG_KC * (COUT / 2); e += blockDim.x) {
+      const int k = e / (COUT / 2), cp = (e % (COUT / 2)) * 2;
+      const int v = base + k;
+      bf16 y0 = __float2bfloat16(0.f), y1 = y0;
+      if (v < total) {
+        y0 = d[(size_t)v * COUT + cp];
+        y1 = d[(size_t)v * COUT + cp + 1];
+      }
+      sb[cp * LD + k] = y0;
+      sb[(cp + 1) * LD + k] = y1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < WG_KC; ks += 16) {
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        const int mb = warp + 4 * m;
+        if (mb >= MB) continue;
+        const bf16* ra = sa + (mb * 16 + g) * LD + ks + 2 * tg;
+        const bf16* rb = sa + (mb * 16 + g + 8) * LD + ks + 2 * tg;
+        const uint32_t a0 = ld32(ra), a1 = ld32(rb), a2 = ld32(ra + 8), a3 = ld32(rb + 8);
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+          const bf16* cb = sb + (j * 8 + g) * LD + ks + 2 * tg;
+          mma16816(acc[m][j], a0, a1, a2, a3, ld32(cb), ld32(cb + 8));
+        }
+      }
+    }
+  }
+  float* out = part + ((size_t)blockIdx.x * 27 + t) * CIN * COUT;
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const int mb = warp + 4 * m;
+    if (mb >= MB) continue;
+#pragma unroll
+    for (int j = 0; j < NT; j++) {
+      const int ci = mb * 16 + g, co = j * 8 + 2 * tg;
+      out[ci * COUT + co] = acc[m][j][0];
+      out[ci * COUT + co + 1] = acc[m][j][1];
+      out[(ci + 8) * COUT + co] = acc[m][j][2];
+      out[(ci + 8) * COUT + co + 1] = acc[m][j][3];
+    }
+  }
+}
+
+// dW[i] = sum over chunks (fixed order) of part[chunk][i]; db[co] = sum of the per-chunk bias sums.
+__global__ void k_wgrad_reduce(const float* part, int nchunk, int n, float* dw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.f;
+  for (int c = 0; c < nchunk; c++) s += part[(size_t)c * n + i];
+  dw[i] = s;
+}
+
+// Bias gradient: db[co] = sum over cells of d[v][co], per-block partials (fixed order) then summed.
+__global__ void k_bgrad_part(Box B, const bf16* d, int cout, float* part) {
+  const int co = threadIdx.x % cout, lanes = blockDim.x / cout, sub = threadIdx.x / cout;
+  const int total = B.total();
+  const int c0 = blockIdx.x * WG_CHUNK;
+  float s = 0.f;
+  for (int v = c0 + sub; v < min(c0 + WG_CHUNK, total); v += lanes) s += __bfloat162float(d[(size_t)v * cout + co]);
+  __shared__ float sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < cout) {
+    float a = 0.f;
+    for (int q = 0; q < lanes; q++) a += sh[q * cout + threadIdx.x];
+    part[(size_t)blockIdx.x * cout + threadIdx.x] = a;
+  }
+}
+
+// 2x2x2 average pooling (fine box F -> coarse box C = F / 2).
+__global__ void k_pool(Box F, Box Cb, const bf16* in, int c, bf16* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Cb.total() * c) return;
+  const int ch = i % c, v = i / c;
+  const int per = Cb.cells(), s = v / per, cc = v % per;
+  const int x = cc % Cb.X, y = (cc / Cb.X) % Cb.Y, z = cc / (Cb.X * Cb.Y);
+  float a = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int fv = s * F.cells() + ((2 * z + (q >> 2)) * F.Y + 2 * y + ((q >> 1) & 1)) * F.X + 2 * x + (q & 1);
+    a += __bfloat162float(in[(size_t)fv * c + ch]);
+  }
+  out[(size_t)v * c + ch] = __float2bfloat16(a * 0.125f);
+}
+
+// Gradient of the pooling: every fine cell gets 1/8 of its parent's gradient, added to dst (fine).
+__global__ void k_pool_bwd_add(Box F, Box Cb, const bf16* dc, int c, bf16* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F.total() * c) return;
+  const int ch = i % c, v = i / c;
+  const int per = F.cells(), s = v / per, cc = v % per;
+  const int x = cc % F.X, y = (cc / F.X) % F.Y, z = cc / (F.X * F.Y);
+  const int pv = s * Cb.cells() + ((z >> 1) * Cb.Y + (y >> 1)) * Cb.X + (x >> 1);
+  const float g = __bfloat162float(dc[(size_t)pv * c + ch]) * 0.125f;
+  dst[i] = __float2bfloat16(__bfloat162float(dst[i]) + g);
+}
+
+// Nearest-neighbour upsampling of a (coarse, cu channels) into channels [0, cu) of a concatenation of
+// width ctot, and the skip tensor (fine, cs channels) into channels [cu, ctot).
+__global__ void k_up_concat(Box F, Box Cb, const bf16* coarse, int cu, const bf16* skip, int cs, bf16* out) {
+  const int ctot = cu + cs;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= F.total() * ctot) return;
+  const int ch = i % ctot, v = i / ctot;
+  if (ch >= cu) {
+    out[i] = skip[(size_t)v * cs + ch - cu];
+    return;
+  }
+  const int per = F.cells(), s = v / per, cc = v % per;
+  const int x = cc % F.X, y = (cc / F.X) % F.Y, z = cc / (F.X * F.Y);
+  const int pv = s * Cb.cells() + ((z >> 1) * Cb.Y + (y >> 1)) * Cb.X + (x >> 1);
+  out[i] = coarse[(size_t)pv * cu + ch];
+}
+
+// Gradient of k_up_concat: the coarse part sums its 8 children (masked by the coarse activation's
+// ReLU), the skip part is added to dskip.
+__global__ void k_up_concat_bwd_coarse(Box F, Box Cb, const bf16* dcat, int cu, int ctot, const bf16* act,
+                                       bf16* dcoarse) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Cb.total() * cu) return;
+  const int ch = i % cu, v = i / cu;
+  const int per = Cb.cells(), s = v / per, cc = v % per;
+  const int x = cc % Cb.X, y = (cc / Cb.X) % Cb.Y, z = cc / (Cb.X * Cb.Y);
+  float a = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int fv = s * F.cells() + ((2 * z + (q >> 2)) * F.Y + 2 * y + ((q >> 1) & 1)) * F.X + 2 * x + (q & 1);
+    a += __bfloat162float(dcat[(size_t)fv * ctot + ch]);
+  }
+  if (!(__bfloat162float(act[i]) > 0.f)) a = 0.f;
+  dcoarse[i] = __float2bfloat16(a);
+}
+
+__global__ void k_concat_bwd_skip(int total, const bf16* dcat, int cu, int ctot, int cs, bf16* dskip) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total * cs) return;
+  const int ch = i % cs, v = i / cs;
+  dskip[i] = dcat[(size_t)v * ctot + cu + ch];
+}
+
+// d = d * (act > 0)
+__global__ void k_relu_mask(int n, bf16* d, const bf16* act) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!(__bfloat162float(act[i]) > 0.f)) d[i] = __float2bfloat16(0.f);
+}
+
+// Per-sample scale s = max |r| over the liquid cells and, with e, the target energy sum e^2.
+__global__ void k_sample_stats(Box B, const uint8_t* cell, const float* r, const float* e, float* scale,
+                               float* energy) {
+  const int s = blockIdx.x;
+  const int per = B.cells();
+  float m = 0.f, en = 0.f;
+  for (int c = threadIdx.x; c < per; c += blockDim.x) {
+    const int v = s * per + c;
+    if ((cell[v] & 3) != FLUID) continue;
+    m = fmaxf(m, fabsf(r[v]));
+    if (e) en += e[v] * e[v];
+  }
+  __shared__ float sm[256], se[256];
+  sm[threadIdx.x] = m;
+  se[threadIdx.x] = en;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = 0.f, b = 0.f;
+    for (int q = 0; q < (int)blockDim.x; q++) {
+      a = fmaxf(a, sm[q]);
+      b += se[q];
+    }
+    scale[s] = a > 0.f ? a : 1.f;
+    if (energy) energy[s] = b > 0.f ? b : 1.f;
+  }
+}
+
+// Network input: [r / s, liquid, air, 0 ...] (16 channels).
+__global__ void k_pack_input(Box B, const uint8_t* cell, const float* r, const float* scale, bf16* x) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= B.total()) return;
+  const int s = v / B.cells();
+  const uint8_t t = cell[v] & 3;
+  bf16 ch[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) ch[q] = __float2bfloat16(0.f);
+  if (t == FLUID) ch[0] = __float2bfloat16(r[v] / scale[s]);
+  ch[1] = __float2bfloat16(t == FLUID ? 1.f : 0.f);
+  ch[2] = __float2bfloat16(t == AIR ? 1.f : 0.f);
+  uint4* dst = reinterpret_cast<uint4*>(x + (size_t)v * 16);
+  dst[0] = *reinterpret_cast<uint4*>(&ch[0]);
+  dst[1] = *reinterpret_cast<uint4*>(&ch[8]);
+}
+
+// Output z = s * o[v][0] on liquid cells.
+__global__ void k_unpack_output(Box B, const uint8_t* cell, const float* o, const float* scale, float* z) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= B.total()) return;
+  const int s = v / B.cells();
+  z[v] = (cell[v] & 3) == FLUID ? scale[s] * o[(size_t)v * 16] : 0.f;
+}
+
+// Relative squared error per sample, L = mean_s sum_liquid (s o - e)^2 / sum e^2, and its gradient
+// with respect to o[v][0] (BF16, 16 channels, the others 0); per-block loss partials.
+__global__ void k_loss(Box B, const uint8_t* cell, const float* o, const float* e, const float* scale,
+                       const float* energy, bf16* dout, float* loss_part) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.f;
+  if (v < B.total()) {
+    const int s = v / B.cells();
+    float g = 0.f;
+    if ((cell[v] & 3) == FLUID) {
+      const float diff = scale[s] * o[(size_t)v * 16] - e[v];
+      l = diff * diff / (energy[s] * B.count);
+      g = 2.f * diff * scale[s] / (energy[s] * B.count);
+    }
+    bf16 ch[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) ch[q] = __float2bfloat16(0.f);
+    ch[0] = __float2bfloat16(g);
+    uint4* dst = reinterpret_cast<uint4*>(dout + (size_t)v * 16);
+    dst[0] = *reinterpret_cast<uint4*>(&ch[0]);
+    dst[1] = *reinterpret_cast<uint4*>(&ch[8]);
+  }
+  __shared__ float sh[256];
+  sh[threadIdx.x] = l;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = 0.f;
+    for (int q = 0; q < (int)blockDim.x; q++) a += sh[q];
+    loss_part[blockIdx.x] = a;
+  }
+}
+
+__global__ void k_sum(const float* part, int n, float* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float a = 0.f;
+  for (int i = 0; i < n; i++) a += part[i];
+  *out = a;
+}
+
+// BF16 weight layouts from the FP32 masters W[t][ci][co]: forward G[t][co][ci] = W[t][ci][co] and
+// data-gradient G[t][ci][co] = W[26 - t][ci][co].
+__global__ void k_prep_weights(const float* w, int cin, int cout, bf16* gf, bf16* gb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 27 * cin * cout) return;
+  const int t = i / (cin * cout), r = i % (cin * cout), ci = r / cout, co = r % cout;
+  gf[((size_t)t * cout + co) * cin + ci] = __float2bfloat16(w[i]);
+  gb[((size_t)(26 - t) * cin + ci) * cout + co] = __float2bfloat16(w[i]);
+}
+
+// Adam (FP32 masters and moments).
+__global__ void k_adam(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1 - b1) * gi, vi = b2 * v[i] + (1 - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+inline unsigned nb(long long n, int t) { return unsigned((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+
+struct UNetImpl {
+  // parameters: per layer W[27][cin][cout] then b[cout], contiguous (FP32 masters)
+  int off_w[NLAYER], off_b[NLAYER];
+  int nparam = 0;
+  float *param = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+  bf16 *gf[NLAYER] = {}, *gb[NLAYER] = {};
+  void* wmem = nullptr;
+  int adam_t = 0;
+  // workspace for one box shape and count
+  Box b1{}, b2{}, b3{};
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  bf16 *x0, *a0, *s1, *p1, *a2, *s2, *p2, *a4, *a5, *c2, *a6, *a7, *c1, *a8, *a9;  // forward
+  bf16 *d_o, *d_a9, *d_a8, *d_c1, *d_a7, *d_a6, *d_c2, *d_a5, *d_a4, *d_p2, *d_s2, *d_a2, *d_p1, *d_s1, *d_a0;
+  float *o, *scale, *energy, *part, *loss_part, *loss;
+  int nchunk = 0, nloss = 0;
+
+  ~UNetImpl() {
+    if (wmem) cudaFree(wmem);
+    if (ws) cudaFree(ws);
+  }
+
+  int init(uint32_t seed, char* err, size_t errlen) {
+    for (int l = 0; l < NLAYER; l++) {
+      off_w[l] = nparam;
+      nparam += 27 * SPEC[l].cin * SPEC[l].cout;
+      off_b[l] = nparam;
+      nparam += SPEC[l].cout;
+    }
+    size_t bf = 0;
+    for (int l = 0; l < NLAYER; l++) bf += 2 * size_t(27) * SPEC[l].cin * SPEC[l].cout;
+    const size_t total = size_t(nparam) * 4 * 4 + bf * 2 + 4096;
+    if (cudaMalloc(&wmem, total) != cudaSuccess) {
+      snprintf(err, errlen, "pl_unet_create: cudaMalloc(%zu) failed", total);
+      wmem = nullptr;
+      return PL_E_NOMEM;
+    }
+    cudaMemset(wmem, 0, total);
+    char* p = static_cast<char*>(wmem);
+    param = (float*)p;
+    grad = param + nparam;
+    m1 = grad + nparam;
+    m2 = m1 + nparam;
+    bf16* q = reinterpret_cast<bf16*>(m2 + nparam);
+    for (int l = 0; l < NLAYER; l++) {
+      gf[l] = q;
+      q += size_t(27) * SPEC[l].cin * SPEC[l].cout;
+      gb[l] = q;
+      q += size_t(27) * SPEC[l].cin * SPEC[l].cout;
+    }
+    // He initialisation from a fixed generator (mulberry32 + Box-Muller); real input channels only
+    std::vector<float> h(nparam, 0.f);
+    uint32_t a = seed;
+    auto uni = [&]() {
+      a += 0x6d2b79f5u;
+      uint32_t t = a;
+      t = (t ^ (t >> 15)) * (t | 1u);
+      t ^= t + (t ^ (t >> 7)) * (t | 61u);
+      return (double(t ^ (t >> 14)) + 0.5) / 4294967296.0;
+    };
+    const int real_in[NLAYER] = {3, 16, 16, 32, 32, 64, 96, 32, 48, 16, 16};
+    const int real_out[NLAYER] = {16, 16, 32, 32, 64, 64, 32, 32, 16, 16, 1};
+    for (int l = 0; l < NLAYER; l++) {
+      const double sd = std::sqrt(2.0 / (27.0 * real_in[l])) * (l == NLAYER - 1 ? 0.1 : 1.0);
+      for (int t = 0; t < 27; t++)
+        for (int ci = 0; ci < real_in[l]; ci++)
+          for (int co = 0; co < real_out[l]; co++) {
+            const double u1 = uni(), u2 = uni();
+            h[off_w[l] + (t * SPEC[l].cin + ci) * SPEC[l].cout + co] =
+                float(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(2 * PI * u2));
+          }
+    }
+    cudaMemcpy(param, h.data(), size_t(nparam) * 4, cudaMemcpyHostToDevice);
+    return cudaGetLastError() == cudaSuccess ? PL_OK : PL_E_CUDA;
+  }
+
+  int workspace(int X, int Y, int Z, int count, char* err, size_t errlen) {
+    if (ws && b1.X == X && b1.Y == Y && b1.Z == Z && b1.count == count) return PL_OK;
+    if (ws) cudaFree(ws);
+    ws = nullptr;
+    b1 = Box{X, Y, Z, count};
+    b2 = Box{X / 2, Y / 2, Z / 2, count};
+    b3 = Box{X / 4, Y / 4, Z / 4, count};
+    const size_t n1 = size_t(b1.total()), n2 = size_t(b2.total()), n3 = size_t(b3.total());
+    nchunk = int((n1 + WG_CHUNK - 1) / WG_CHUNK);
+    nloss = int((n1 + 255) / 256);
+    size_t maxw = 0;
+    for (int l = 0; l < NLAYER; l++) maxw = std::max(maxw, size_t(27) * SPEC[l].cin * SPEC[l].cout);
+    std::vector<size_t> sz = {
+        n1 * 16, n1 * 16, n1 * 16, n2 * 16, n2 * 32, n2 * 32, n3 * 32, n3 * 64, n3 * 64, n2 * 96, n2 * 32, n2 * 32,
+        n1 * 48, n1 * 16, n1 * 16,                                                               // forward (bf16 elems)
+        n1 * 16, n1 * 16, n1 * 16, n1 * 48, n2 * 32, n2 * 32, n2 * 96, n3 * 64, n3 * 64, n3 * 32, n2 * 32, n2 * 32,
+        n2 * 16, n1 * 16, n1 * 16};                                                              // gradients
+    size_t bytes = 0;
+    for (size_t s : sz) bytes += ((s * 2 + 255) & ~size_t(255));
+    const size_t fbytes = n1 * 16 * 4 + 2 * size_t(count) * 4 + size_t(nchunk) * maxw * 4 + size_t(nloss) * 4 + 1024;
+    if (cudaMalloc(&ws, bytes + fbytes + 4096) != cudaSuccess) {
+      ws = nullptr;
+      snprintf(err, errlen, "pl_unet: workspace cudaMalloc(%zu) failed", bytes + fbytes);
+      return PL_E_NOMEM;
+    }
+    ws_bytes = bytes + fbytes;
+    char* p = static_cast<char*>(ws);
+    std::vector<bf16*> ptr;
+    for (size_t s : sz) {
+      ptr.push_back((bf16*)p);
+      p += (s * 2 + 255) & ~size_t(255);
+    }
+    bf16** fw[] = {&x0, &a0, &s1, &p1, &a2, &s2, &p2, &a4, &a5, &c2, &a6, &a7, &c1, &a8, &a9,
+                   &d_o, &d_a9, &d_a8, &d_c1, &d_a7, &d_a6, &d_c2, &d_a5, &d_a4, &d_p2, &d_s2, &d_a2, &d_p1, &d_s1, &d_a0};
+    for (size_t i = 0; i < ptr.size(); i++) *fw[i] = ptr[i];
+    o = (float*)p;
+    p += n1 * 16 * 4;
+    scale = (float*)p;
+    p += size_t(count) * 4;
+    energy = (float*)p;
+    p += size_t(count) * 4;
+    p = (char*)(((uintptr_t)p + 255) & ~uintptr_t(255));
+    part = (float*)p;
+    p += size_t(nchunk) * maxw * 4;
+    loss_part = (float*)p;
+    p += size_t(nloss) * 4;
+    loss = (float*)p;
+    return PL_OK;
+  }
+
+  void prep_weights(cudaStream_t st) {
+    for (int l = 0; l < NLAYER; l++) {
+      const int n = 27 * SPEC[l].cin * SPEC[l].cout;
+      k_prep_weights<<<nb(n, 256), 256, 0, st>>>(param + off_w[l], SPEC[l].cin, SPEC[l].cout, gf[l], gb[l]);
+    }
+  }
+
+  // out = conv_l(in) (forward, G = gf) or the data gradient (G = gb; then nout = cin of the layer).
+  void conv(const Box& B, const bf16* in, int cin, const bf16* G, int nout, const float* bias, int relu,
+            const bf16* mask, bf16* out_bf, float* out_f32, cudaStream_t st) {
+    const long long warps = (B.total() + 15) / 16;
+    const unsigned blocks = nb(warps * 32, 128);
+    if (nout == 16)
+      k_conv<16><<<blocks, 128, 0, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32);
+    else if (nout == 32)
+      k_conv<32><<<blocks, 128, 0, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32);
+    else if (nout == 48)
+      k_conv<48><<<blocks, 128, 0, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32);
+    else if (nout == 64)
+      k_conv<64><<<blocks, 128, 0, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32);
+    else
+      k_conv<96><<<blocks, 128, 0, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32);
+  }
+
+  void forward(const uint8_t* cell, const float* r, cudaStream_t st) {
+    prep_weights(st);
+    k_sample_stats<<<b1.count, 256, 0, st>>>(b1, cell, r, nullptr, scale, nullptr);
+    k_pack_input<<<nb(b1.total(), 256), 256, 0, st>>>(b1, cell, r, scale, x0);
+    auto L = [&](int l, const Box& B, const bf16* in, bf16* out, int relu, float* f32) {
+      conv(B, in, SPEC[l].cin, gf[l], SPEC[l].cout, param + off_b[l], relu, nullptr, out, f32, st);
+    };
+    L(0, b1, x0, a0, 1, nullptr);
+    L(1, b1, a0, s1, 1, nullptr);
+    k_pool<<<nb((long long)b2.total() * 16, 256), 256, 0, st>>>(b1, b2, s1, 16, p1);
+    L(2, b2, p1, a2, 1, nullptr);
+    L(3, b2, a2, s2, 1, nullptr);
+    k_pool<<<nb((long long)b3.total() * 32, 256), 256, 0, st>>>(b2, b3, s2, 32, p2);
+    L(4, b3, p2, a4, 1, nullptr);
+    L(5, b3, a4, a5, 1, nullptr);
+    k_up_concat<<<nb((long long)b2.total() * 96, 256), 256, 0, st>>>(b2, b3, a5, 64, s2, 32, c2);
+    L(6, b2, c2, a6, 1, nullptr);
+    L(7, b2, a6, a7, 1, nullptr);
+    k_up_concat<<<nb((long long)b1.total() * 48, 256), 256, 0, st>>>(b1, b2, a7, 32, s1, 16, c1);
+    L(8, b1, c1, a8, 1, nullptr);
+    L(9, b1, a8, a9, 1, nullptr);
+    L(10, b1, a9, nullptr, 0, o);
+  }
+
+  // Weight and bias gradient of layer l from its input and the gradient of its pre-activation.
+  void wgrad(int l, const Box& B, const bf16* in, const bf16* d, cudaStream_t st) {
+    const int ci = SPEC[l].cin, co = SPEC[l].cout;
+    const int nch = (B.total() + WG_CHUNK - 1) / WG_CHUNK;
+    dim3 grid(nch, 27);
+#define WG(CI, CO) \
+  if (ci == CI && co == CO) k_wgrad<CI, CO><<<grid, 128, 0, st>>>(B, in, d, part);
+    WG(16, 16) WG(16, 32) WG(32, 32) WG(32, 64) WG(64, 64) WG(96, 32) WG(48, 16)
+#undef WG
+    const int n = 27 * ci * co;
+    k_wgrad_reduce<<<nb(n, 256), 256, 0, st>>>(part, nch, n, grad + off_w[l]);
+    k_bgrad_part<<<nch, (256 / co) * co, 0, st>>>(B, d, co, part);
+    k_wgrad_reduce<<<1, 256, 0, st>>>(part, nch, co, grad + off_b[l]);
+  }
+
+  // Data gradient through layer l: din = conv^T(d) masked by the ReLU of mask (null: no mask).
+  void dgrad(int l, const Box& B, const bf16* d, const bf16* mask, bf16* din, cudaStream_t st) {
+    conv(B, d, SPEC[l].cout, gb[l], SPEC[l].cin, nullptr, 0, mask, din, nullptr, st);
+  }
+
+  void backward(cudaStream_t st) {
+    // d_o holds dL/do (channel 0); ReLU-free output layer
+    wgrad(10, b1, a9, d_o, st);
+    dgrad(10, b1, d_o, a9, d_a9, st);
+    wgrad(9, b1, a8, d_a9, st);
+    dgrad(9, b1, d_a9, a8, d_a8, st);
+    wgrad(8, b1, c1, d_a8, st);
+    dgrad(8, b1, d_a8, nullptr, d_c1, st);
+    k_up_concat_bwd_coarse<<<nb((long long)b2.total() * 32, 256), 256, 0, st>>>(b1, b2, d_c1, 32, 48, a7, d_a7);
+    k_concat_bwd_skip<<<nb((long long)b1.total() * 16, 256), 256, 0, st>>>(b1.total(), d_c1, 32, 48, 16, d_s1);
+    wgrad(7, b2, a6, d_a7, st);
+    dgrad(7, b2, d_a7, a6, d_a6, st);
+    wgrad(6, b2, c2, d_a6, st);
+    dgrad(6, b2, d_a6, nullptr, d_c2, st);
+    k_up_concat_bwd_coarse<<<nb((long long)b3.total() * 64, 256), 256, 0, st>>>(b2, b3, d_c2, 64, 96, a5, d_a5);
+    k_concat_bwd_skip<<<nb((long long)b2.total() * 32, 256), 256, 0, st>>>(b2.total(), d_c2, 64, 96, 32, d_s2);
+    wgrad(5, b3, a4, d_a5, st);
+    dgrad(5, b3, d_a5, a4, d_a4, st);
+    wgrad(4, b3, p2, d_a4, st);
+    dgrad(4, b3, d_a4, nullptr, d_p2, st);
+    k_pool_bwd_add<<<nb((long long)b2.total() * 32, 256), 256, 0, st>>>(b2, b3, d_p2, 32, d_s2);
+    k_relu_mask<<<nb((long long)b2.total() * 32, 256), 256, 0, st>>>(b2.total() * 32, d_s2, s2);
+    wgrad(3, b2, a2, d_s2, st);
+    dgrad(3, b2, d_s2, a2, d_a2, st);
+    wgrad(2, b2, p1, d_a2, st);
+    dgrad(2, b2, d_a2, nullptr, d_p1, st);
+    k_pool_bwd_add<<<nb((long long)b1.total() * 16, 256), 256, 0, st>>>(b1, b2, d_p1, 16, d_s1);
+    k_relu_mask<<<nb((long long)b1.total() * 16, 256), 256, 0, st>>>(b1.total() * 16, d_s1, s1);
+    wgrad(1, b1, a0, d_s1, st);
+    dgrad(1, b1, d_s1, a0, d_a0, st);
+    wgrad(0, b1, x0, d_a0, st);
+  }
+
+  void loss_and_grad(const uint8_t* cell, const float* e, cudaStream_t st) {
+    k_sample_stats<<<b1.count, 256, 0, st>>>(b1, cell, e, e, part, energy);  // energy of the targets
+    k_loss<<<nb(b1.total(), 256), 256, 0, st>>>(b1, cell, o, e, scale, energy, d_o, loss_part);
+    k_sum<<<1, 32, 0, st>>>(loss_part, nloss, loss);
+  }
+};
+
+namespace {
+int check_box(int X, int Y, int Z, int count, char* err, size_t errlen) {
+  if (X < 4 || Y < 4 || Z < 4 || X % 4 || Y % 4 || Z % 4 || count < 1 ||
+      (long long)X * Y * Z * count > (1ll << 26)) {
+    snprintf(err, errlen, "pl_unet: box %dx%dx%d x %d must be multiples of 4 with at most 2^26 cells", X, Y, Z,
+             count);
+    return PL_E_ARG;
+  }
+  return PL_OK;
+}
+}  // namespace
+
+UNetImpl* unet_create(uint32_t seed, char* err, size_t errlen, int* rc) {
+  UNetImpl* u = new UNetImpl();
+  *rc = u->init(seed, err, errlen);
+  if (*rc) {
+    delete u;
+    return nullptr;
+  }
+  return u;
+}
+
+void unet_destroy(UNetImpl* u) { delete u; }
+
+int unet_nparams(const UNetImpl* u) { return u->nparam; }
+
+int unet_get_params(UNetImpl* u, float* host) {
+  return cudaMemcpy(host, u->param, size_t(u->nparam) * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? PL_OK
+                                                                                                   : PL_E_CUDA;
+}
+
+int unet_set_params(UNetImpl* u, const float* host) {
+  u->adam_t = 0;
+  cudaMemset(u->m1, 0, size_t(u->nparam) * 4);
+  cudaMemset(u->m2, 0, size_t(u->nparam) * 4);
+  return cudaMemcpy(u->param, host, size_t(u->nparam) * 4, cudaMemcpyHostToDevice) == cudaSuccess ? PL_OK
+                                                                                                   : PL_E_CUDA;
+}
+
+int unet_apply(UNetImpl* u, const uint8_t* cell, const float* r, float* z, int X, int Y, int Z, int count,
+               cudaStream_t st, char* err, size_t errlen) {
+  int rc = check_box(X, Y, Z, count, err, errlen);
+  if (!rc) rc = u->workspace(X, Y, Z, count, err, errlen);
+  if (rc) return rc;
+  u->forward(cell, r, st);
+  k_unpack_output<<<nb(u->b1.total(), 256), 256, 0, st>>>(u->b1, cell, u->o, u->scale, z);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    snprintf(err, errlen, "pl_unet_apply: %s", cudaGetErrorString(e));
+    return PL_E_CUDA;
+  }
+  return PL_OK;
+}
+
+int unet_gradient(UNetImpl* u, const uint8_t* cell, const float* r, const float* e, int X, int Y, int Z, int count,
+                  float lr, int update, float* loss, float* grad_host, cudaStream_t st, char* err, size_t errlen) {
+  int rc = check_box(X, Y, Z, count, err, errlen);
+  if (!rc) rc = u->workspace(X, Y, Z, count, err, errlen);
+  if (rc) return rc;
+  u->forward(cell, r, st);
+  u->loss_and_grad(cell, e, st);
+  u->backward(st);
+  if (update) {
+    u->adam_t++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    k_adam<<<nb(u->nparam, 256), 256, 0, st>>>(u->nparam, u->param, u->grad, u->m1, u->m2, lr, b1, b2, 1e-8f,
+                                               1.f - std::pow(b1, float(u->adam_t)),
+                                               1.f - std::pow(b2, float(u->adam_t)));
+  }
+  cudaError_t ce = cudaMemcpyAsync(loss, u->loss, 4, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess && grad_host)
+    ce = cudaMemcpyAsync(grad_host, u->grad, size_t(u->nparam) * 4, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess) {
+    snprintf(err, errlen, "pl_unet: %s", cudaGetErrorString(ce));
+    return PL_E_CUDA;
+  }
+  return PL_OK;
+}
+
+}  // namespace pl

@@ -28,7 +28,9 @@ EXPORTED = [
     "pl_read_particles_f64", "pl_read_origin", "pl_read_render_positions", "pl_get_state", "pl_set_state",
     "pl_get_field", "pl_pcg_solve_device", "pl_enqueue_substeps", "pl_stream", "pl_enable_stage_timing",
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
-    "pl_get_affine", "pl_set_affine", "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
+    "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
+    "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
+    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -92,6 +94,16 @@ def lib() -> C.CDLL:
     L.pl_stream.restype = C.c_void_p
     L.pl_enable_stage_timing.argtypes = [P, C.c_int32]
     L.pl_stage_times.argtypes = [P, fp]
+    L.pl_unet_create.argtypes = [C.c_uint32, C.POINTER(P)]
+    L.pl_unet_num_params.argtypes = [P]
+    L.pl_unet_num_params.restype = C.c_int32
+    L.pl_unet_get_params.argtypes = [P, fp]
+    L.pl_unet_set_params.argtypes = [P, fp]
+    L.pl_unet_apply.argtypes = [P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P]
+    L.pl_unet_train_step.argtypes = [P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, fp, P]
+    L.pl_unet_gradient.argtypes = [P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, fp, P]
+    L.pl_unet_destroy.argtypes = [P]
+    L.pl_unet_destroy.restype = None
     L.pl_get_affine.argtypes = [P, fp]
     L.pl_set_affine.argtypes = [P, fp]
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
@@ -410,6 +422,60 @@ class PoissonBatch:
     def destroy(self):
         if self._h:
             lib().pl_poisson_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ learned preconditioner
+
+UNET_LAYERS = [(16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32), (32, 32), (48, 16), (16, 16),
+               (16, 16)]  # (input, output) channels of the 11 convolutions, padded to multiples of 16
+
+
+class UNet:
+    """The learned preconditioner's network (pl_unet_*) on device pointers (cell u8, r/z/e f32)."""
+
+    def __init__(self, seed: int = 1):
+        h = C.c_void_p()
+        _check(lib().pl_unet_create(seed, C.byref(h)))
+        self._h = h
+        self.nparams = int(lib().pl_unet_num_params(h))
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.nparams, np.float32)
+        _check(lib().pl_unet_get_params(self._h, _ptr(out, C.c_float)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        _check(lib().pl_unet_set_params(self._h, _ptr(p, C.c_float)))
+
+    def apply(self, cell_ptr: int, r_ptr: int, z_ptr: int, nx: int, ny: int, nz: int, count: int, stream: int = 0):
+        _check(lib().pl_unet_apply(self._h, C.c_void_p(cell_ptr), C.c_void_p(r_ptr), C.c_void_p(z_ptr), nx, ny, nz,
+                                   count, C.c_void_p(stream)))
+
+    def train_step(self, cell_ptr, r_ptr, e_ptr, nx, ny, nz, count, lr: float, stream: int = 0) -> float:
+        loss = C.c_float(0)
+        _check(lib().pl_unet_train_step(self._h, C.c_void_p(cell_ptr), C.c_void_p(r_ptr), C.c_void_p(e_ptr), nx, ny,
+                                        nz, count, lr, C.byref(loss), C.c_void_p(stream)))
+        return float(loss.value)
+
+    def gradient(self, cell_ptr, r_ptr, e_ptr, nx, ny, nz, count, stream: int = 0) -> tuple[float, np.ndarray]:
+        loss = C.c_float(0)
+        g = np.zeros(self.nparams, np.float32)
+        _check(lib().pl_unet_gradient(self._h, C.c_void_p(cell_ptr), C.c_void_p(r_ptr), C.c_void_p(e_ptr), nx, ny,
+                                      nz, count, C.byref(loss), _ptr(g, C.c_float), C.c_void_p(stream)))
+        return float(loss.value), g
+
+    def destroy(self):
+        if self._h:
+            lib().pl_unet_destroy(self._h)
             self._h = None
 
     def __del__(self):

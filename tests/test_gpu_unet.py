@@ -1,0 +1,72 @@
+"""The learned preconditioner's U-Net kernels (BF16 tensor-core convolutions, FP32 accumulation) against
+the CPU FP64 restatement in unet_ref.py: the forward output, the loss and every layer's gradient."""
+import numpy as np
+import pytest
+import torch
+
+import unet_ref
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ, N = 16, 12, 8, 2
+
+
+def case(seed=3):
+    rng = np.random.default_rng(seed)
+    cell = np.full((N, NZ, NY, NX), 2, np.uint8)
+    cell[:, 1:-1, 1:-1, 1:-1] = 0
+    cell[:, 1:-1, 1:7, 1:-1] = 1                      # a liquid slab under air
+    cell[1, 2:5, 7:10, 3:9] = 1                       # and a blob in the second box
+    r = (rng.standard_normal(cell.shape) * (cell == 1)).astype(np.float32)
+    e = (rng.standard_normal(cell.shape) * (cell == 1)).astype(np.float32)
+    return cell, r, e
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_forward_matches_fp64_restatement(engine):
+    cell, r, e = case()
+    net = engine.engine.UNet(seed=5)
+    p = net.params()
+    dc, dr = dev(cell), dev(r)
+    dz = torch.zeros_like(dr)
+    net.apply(dc.data_ptr(), dr.data_ptr(), dz.data_ptr(), NX, NY, NZ, N)
+    torch.cuda.synchronize()
+    z = dz.cpu().numpy().astype(np.float64)
+    zr, _ = unet_ref.forward(unet_ref.unpack(p), cell, r)
+    zr = zr.detach().numpy()
+    assert np.all(z[cell != 1] == 0)
+    rel = np.linalg.norm(z - zr) / np.linalg.norm(zr)
+    assert rel < 3e-2, rel  # BF16 weights and activations through 11 layers
+
+
+def test_gradient_matches_fp64_restatement(engine):
+    cell, r, e = case()
+    net = engine.engine.UNet(seed=5)
+    p = net.params()
+    dc, dr, de = dev(cell), dev(r), dev(e)
+    loss, g = net.gradient(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), NX, NY, NZ, N)
+    loss_ref, g_ref, _ = unet_ref.loss_and_grad(p.astype(np.float64), cell, r, e)
+    assert abs(loss - loss_ref) < 2e-2 * abs(loss_ref)
+    cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
+    assert cos > 0.995, cos
+    o = 0
+    for li, (ci, co) in enumerate(unet_ref.LAYERS):
+        n = 27 * ci * co + co
+        a, b = g[o:o + n], g_ref[o:o + n]
+        o += n
+        if np.linalg.norm(b) > 0:
+            assert np.linalg.norm(a - b) <= 0.1 * np.linalg.norm(b), (li, np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_training_lowers_the_loss(engine):
+    cell, r, e = case(7)
+    net = engine.engine.UNet(seed=9)
+    dc, dr, de = dev(cell), dev(r), dev(e)
+    first = net.train_step(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), NX, NY, NZ, N, 1e-3)
+    last = first
+    for _ in range(60):
+        last = net.train_step(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), NX, NY, NZ, N, 1e-3)
+    assert last < 0.7 * first, (first, last)
