@@ -394,7 +394,11 @@ typedef struct pl_poisson pl_poisson;
  * vectors, FP64 inner products, norms, solution and true-residual refinement; PL_SOLVE_F64: all
  * FP64). Holds its device scratch until pl_poisson_destroy. */
 int pl_poisson_create(int32_t n, int32_t count, int32_t method, int32_t precision, pl_poisson** out);
-/* Solve every snapshot (device buffers: cell u8, b f32 and x f64, each count * n^3) on stream with
+/* The same for boxes of nx x ny x nz cells (each a power of two in [8, 512]); the multigrid halves every
+ * axis longer than 8 per level (semi-coarsening on thin boxes). */
+int pl_poisson_create_box(int32_t nx, int32_t ny, int32_t nz, int32_t count, int32_t method, int32_t precision,
+                          pl_poisson** out);
+/* Solve every snapshot (device buffers: cell u8, b f32 and x f64, each count * cells) on stream with
  * the reference's stopping rule (max-norm residual <= max(tol * max|b|, 1e-14), at most max_iter
  * iterations); writes per-snapshot iterations, final max-norm residual and converged flag to host
  * arrays of count entries (any may be NULL). Synchronous. */

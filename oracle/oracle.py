@@ -57,6 +57,8 @@ def lib() -> C.CDLL:
         L.plo_get_affine.argtypes = [P, dp]
         L.plo_set_affine.argtypes = [P, dp]
         L.plo_poisson_solve.argtypes = [u8p, dp, dp, C.c_int32, C.c_double, C.c_int32, C.POINTER(C.c_int32), dp]
+        L.plo_poisson_solve_box.argtypes = [u8p, dp, dp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                            C.POINTER(C.c_int32), dp]
         L.plo_teapot_sdf.argtypes = [C.POINTER(abi.Teapot), C.c_double, C.c_double, C.c_double]
         L.plo_teapot_sdf.restype = C.c_double
         L.plo_in_cavity.argtypes = [C.POINTER(abi.Teapot), C.c_double, C.c_double, C.c_double]
@@ -209,16 +211,18 @@ def pcg_solve(cell: np.ndarray, b: np.ndarray, nx: int, ny: int, nz: int, tol: f
     return q, it, bool(conv.value), res.value
 
 
-def poisson_solve(cell: np.ndarray, b: np.ndarray, n: int, tol: float = 1e-12, max_iter: int = 4000):
-    """FP64 MIC(0)-PCG of one dense Poisson snapshot (cells may carry the pin flag 4)."""
+def poisson_solve(cell: np.ndarray, b: np.ndarray, n, tol: float = 1e-12, max_iter: int = 4000):
+    """FP64 MIC(0)-PCG of one dense Poisson snapshot (cells may carry the pin flag 4); n is the cube's edge
+    or (nx, ny, nz)."""
     L = lib()
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else tuple(n)
     cell = np.ascontiguousarray(cell, np.uint8)
     b = np.ascontiguousarray(b, np.float64)
-    q = np.zeros(n * n * n)
+    q = np.zeros(nx * ny * nz)
     conv = C.c_int32(0)
     res = C.c_double(0)
-    it = L.plo_poisson_solve(_ptr(cell, C.c_uint8), _ptr(b, C.c_double), _ptr(q, C.c_double), n, tol, max_iter,
-                             C.byref(conv), C.byref(res))
+    it = L.plo_poisson_solve_box(_ptr(cell, C.c_uint8), _ptr(b, C.c_double), _ptr(q, C.c_double), nx, ny, nz, tol,
+                                 max_iter, C.byref(conv), C.byref(res))
     return q, it, bool(conv.value), res.value
 
 

@@ -1340,25 +1340,30 @@ int plo_pcg_solve(const uint8_t* cell, const double* b, double* q, int32_t nx, i
 
 // One snapshot of the Poisson batch: cells may carry PL_POISSON_PIN on FLUID cells (diagonal + 1);
 // FLUID cells on the grid border are not unknowns. FP64 Pcg3D.solve with MIC(0).
-int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,
-                      int32_t* converged, double* residual) {
-  const size_t nc = size_t(n) * n * n;
+int plo_poisson_solve_box(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny, int32_t nz,
+                          double tol, int32_t max_iter, int32_t* converged, double* residual) {
+  const size_t nc = size_t(nx) * ny * nz;
   std::vector<uint8_t> base(nc), pin(nc);
-  for (int k = 0; k < n; k++)
-    for (int j = 0; j < n; j++)
-      for (int i = 0; i < n; i++) {
-        const size_t c = (size_t(k) * n + j) * n + i;
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        const size_t c = (size_t(k) * ny + j) * nx + i;
         uint8_t t = cell[c] & 3;
-        const bool border = i == 0 || j == 0 || k == 0 || i == n - 1 || j == n - 1 || k == n - 1;
+        const bool border = i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1;
         if (border && t == FLUID) t = AIR;  // a border FLUID cell is not an unknown: Dirichlet, like AIR
         base[c] = t;
         pin[c] = (t == FLUID && (cell[c] & 4)) ? 1 : 0;
       }
-  Pcg3D pcg(n, n, n);
+  Pcg3D pcg(nx, ny, nz);
   SolveResult r = pcg.solve(base.data(), nc, b, q, tol, max_iter, pin.data());
   if (converged) *converged = r.converged ? 1 : 0;
   if (residual) *residual = r.residual;
   return r.iterations;
+}
+
+int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,
+                      int32_t* converged, double* residual) {
+  return plo_poisson_solve_box(cell, b, q, n, n, n, tol, max_iter, converged, residual);
 }
 
 void plo_get_affine(const plo_sim* s, double* c9) {

@@ -53,6 +53,9 @@ void plo_set_affine(plo_sim* s, const double* c9);
  * fix of src/sim/pressure.ts:232-268); FP64 MIC(0)-PCG as Pcg3D.solve. Returns the iterations. */
 int plo_poisson_solve(const uint8_t* cell, const double* b, double* q, int32_t n, double tol, int32_t max_iter,
                       int32_t* converged, double* residual);
+/* The same on a box of nx x ny x nz cells. */
+int plo_poisson_solve_box(const uint8_t* cell, const double* b, double* q, int32_t nx, int32_t ny, int32_t nz,
+                          double tol, int32_t max_iter, int32_t* converged, double* residual);
 
 /* Geometry (vessel3d.ts:46-103) for unit tests. */
 double plo_teapot_sdf(const pl_teapot* t, double x, double y, double z);

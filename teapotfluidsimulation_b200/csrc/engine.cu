@@ -931,26 +931,32 @@ int pl_poisson_gauge_fix(int32_t n, int32_t count, uint8_t* cell, float* b, int3
   return PL_OK;
 }
 
-int pl_poisson_create(int32_t n, int32_t count, int32_t method, int32_t precision, pl_poisson** out) {
+int pl_poisson_create_box(int32_t nx, int32_t ny, int32_t nz, int32_t count, int32_t method, int32_t precision,
+                          pl_poisson** out) {
   if (!out) return fail(PL_E_ARG, "pl_poisson_create: null argument");
   *out = nullptr;
-  if (n < 8 || n > 512 || (n & (n - 1)) || count < 1)
-    return fail(PL_E_ARG, "pl_poisson_create: n must be a power of two in [8, 512] and count >= 1 (n=%d count=%d)", n,
-                count);
+  auto pow2 = [](int v) { return v >= 8 && v <= 512 && (v & (v - 1)) == 0; };
+  if (!pow2(nx) || !pow2(ny) || !pow2(nz) || count < 1)
+    return fail(PL_E_ARG, "pl_poisson_create: box extents must be powers of two in [8, 512] and count >= 1 "
+                "(%dx%dx%d, count=%d)", nx, ny, nz, count);
   if (method != PL_POISSON_MIC0 && method != PL_POISSON_MG)
     return fail(PL_E_ARG, "pl_poisson_create: unknown method %d", method);
   if (precision != PL_SOLVE_F64 && precision != PL_SOLVE_MIXED)
     return fail(PL_E_ARG, "pl_poisson_create: unknown precision %d", precision);
-  if ((long long)n * n * n * count > (1ll << 31) - 1)
-    return fail(PL_E_ARG, "pl_poisson_create: %d snapshots of %d^3 cells exceed 2^31 cells", count, n);
+  if ((long long)nx * ny * nz * count > (1ll << 31) - 1)
+    return fail(PL_E_ARG, "pl_poisson_create: %d boxes of %dx%dx%d cells exceed 2^31 cells", count, nx, ny, nz);
   char err[256] = "";
   int rc = 0;
-  pl::PoissonImpl* impl = pl::poisson_create(n, count, method, precision, err, sizeof err, &rc);
+  pl::PoissonImpl* impl = pl::poisson_create(nx, ny, nz, count, method, precision, err, sizeof err, &rc);
   if (!impl) return fail(rc ? rc : PL_E_CUDA, "%s", err);
-  pl_poisson* h = new pl_poisson{impl, n, count, 0};
+  pl_poisson* h = new pl_poisson{impl, nx, count, 0};
   cudaGetDevice(&h->device);
   *out = h;
   return PL_OK;
+}
+
+int pl_poisson_create(int32_t n, int32_t count, int32_t method, int32_t precision, pl_poisson** out) {
+  return pl_poisson_create_box(n, n, n, count, method, precision, out);
 }
 
 int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double* x, double tol, int32_t max_iter,

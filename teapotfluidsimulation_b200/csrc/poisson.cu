@@ -61,13 +61,14 @@ constexpr double MG_OMEGA = 1.5;   // over-relaxation of the coarse correction
 constexpr uint8_t C_SELF = 1u << 6;
 
 struct TG {  // tiling of one level (every extent a power of two)
-  int n;
+  int nx, ny, nz;     // cells per axis
+  int rx, ry, rz;     // coarsening factor (1 or 2) from the finer level on each axis (1 on level 0)
   int tx, ty, tz;     // tile extent
   int px, py, pz;     // tiles per axis
   long long nc;       // cells per snapshot
   long long ntile;    // tiles per snapshot
   // base-2 logarithms for the index arithmetic (all indices fit in 32 bits: checked at creation)
-  int ln, ltx, lty, lpx, lpy, lnt, lnc;
+  int lnx, lny, ltx, lty, lpx, lpy, lnt, lnc;
 };
 
 inline int ilog2(long long v) {
@@ -76,19 +77,20 @@ inline int ilog2(long long v) {
   return l;
 }
 
-TG make_tg(int n) {
+TG make_tg(int nx, int ny, int nz, int rx = 1, int ry = 1, int rz = 1) {
   TG t;
-  t.n = n;
-  t.tx = std::min(32, n);
-  t.ty = std::min(4, n);
-  t.tz = PT / (t.tx * t.ty);
-  if (t.tz > n) t.tz = n;
-  t.px = n / t.tx;
-  t.py = n / t.ty;
-  t.pz = n / t.tz;
-  t.nc = (long long)n * n * n;
+  t.nx = nx, t.ny = ny, t.nz = nz;
+  t.rx = rx, t.ry = ry, t.rz = rz;
+  t.tx = std::min(32, nx);
+  t.ty = std::min(4, ny);
+  t.tz = PT / (t.tx * t.ty);  // every extent is >= 8, so a tile always holds PT cells
+  t.px = nx / t.tx;
+  t.py = ny / t.ty;
+  t.pz = nz / t.tz;
+  t.nc = (long long)nx * ny * nz;
   t.ntile = (long long)t.px * t.py * t.pz;
-  t.ln = ilog2(n);
+  t.lnx = ilog2(nx);
+  t.lny = ilog2(ny);
   t.ltx = ilog2(t.tx);
   t.lty = ilog2(t.ty);
   t.lpx = ilog2(t.px);
@@ -107,7 +109,7 @@ __device__ __forceinline__ bool tile_cell(const TG& G, int gt, int tid, int& s, 
   i = (ti << G.ltx) + (tid & (G.tx - 1));
   j = (tj << G.lty) + ((tid >> G.ltx) & (G.ty - 1));
   k = (tk * G.tz) + (tid >> (G.ltx + G.lty));
-  c = (s << G.lnc) + (((k << G.ln) + j) << G.ln) + i;
+  c = (s << G.lnc) + (((k << G.lny) + j) << G.lnx) + i;
   return true;
 }
 
@@ -139,20 +141,20 @@ __global__ void k_lvl_code(TG G, const uint8_t* type, uint8_t* code, uint8_t* di
   int c;
   bool any = false;
   if (gt < (long long)count * G.ntile && tile_cell(G, gt, threadIdx.x, s, i, j, k, c)) {
-    const int n = G.n;
-    const int nxy = n * n;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const int nxy = nx * ny;
     const uint8_t t = type[c];
-    const bool interior = i > 0 && j > 0 && k > 0 && i < n - 1 && j < n - 1 && k < n - 1;
+    const bool interior = i > 0 && j > 0 && k > 0 && i < nx - 1 && j < ny - 1 && k < nz - 1;
     uint8_t cd = 0, d = 0;
     if (interior && base_type(t) == FLUID) {
-      const int off[6] = {-1, 1, -n, n, -nxy, nxy};
+      const int off[6] = {-1, 1, -nx, nx, -nxy, nxy};
       const int nb[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
 #pragma unroll
       for (int f = 0; f < 6; f++) {
         const uint8_t tn = base_type(type[c + off[f]]);
         if (tn != SOLID) d++;
-        const bool nin = nb[f][0] > 0 && nb[f][1] > 0 && nb[f][2] > 0 && nb[f][0] < n - 1 && nb[f][1] < n - 1 &&
-                         nb[f][2] < n - 1;
+        const bool nin = nb[f][0] > 0 && nb[f][1] > 0 && nb[f][2] > 0 && nb[f][0] < nx - 1 && nb[f][1] < ny - 1 &&
+                         nb[f][2] < nz - 1;
         if (tn == FLUID && nin) cd |= uint8_t(1u << f);
       }
       cd |= C_SELF;
@@ -166,7 +168,7 @@ __global__ void k_lvl_code(TG G, const uint8_t* type, uint8_t* code, uint8_t* di
   if (threadIdx.x == 0 && gt < (long long)count * G.ntile) flag[gt] = any ? 1 : 0;
 }
 
-// Galerkin coarse level l+1 from level l (A_c = P^T A P for 2 x 2 x 2 aggregates): unknown if any
+// Galerkin coarse level l+1 from level l (A_c = P^T A P for rx x ry x rz aggregates): unknown if any
 // child is; link weight to the aggregate across face f = sum of the children's links across it;
 // diagonal = sum of the children's diagonals minus the links inside the aggregate. wf == nullptr:
 // the fine level is level 0 (unit links from its code bits, diagonal bytes).
@@ -179,19 +181,21 @@ __global__ void k_gal_coarsen(TG Gf, TG Gc, const uint8_t* codef, const uint8_t*
   bool any = false;
   const int cellsf = int(count * Gf.nc), cellsc = int(count * Gc.nc);
   if (gt < (long long)count * Gc.ntile && tile_cell(Gc, gt, threadIdx.x, s, i, j, k, c)) {
-    const int nf = Gf.n;
+    const int rx = Gc.rx, ry = Gc.ry, rz = Gc.rz;
     T w6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
     T d = T(0);
     bool u = false;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       const int dx = q & 1, dy = (q >> 1) & 1, dz = q >> 2;
-      const int cf = (s << Gf.lnc) + (((2 * k + dz) * nf + 2 * j + dy) * nf) + 2 * i + dx;
+      if (dx >= rx || dy >= ry || dz >= rz) continue;
+      const int cf = (s << Gf.lnc) + ((rz * k + dz) * Gf.ny + ry * j + dy) * Gf.nx + rx * i + dx;
       const uint8_t cd = codef[cf];
       if (!(cd & C_SELF)) continue;
       u = true;
       d += wf ? dgf[cf] : T(diagf[cf]);
-      const int side[6] = {dx == 0, dx == 1, dy == 0, dy == 1, dz == 0, dz == 1};  // link leaves the aggregate
+      // the link leaves the aggregate (on an axis that is not coarsened both links leave)
+      const int side[6] = {dx == 0, dx == rx - 1, dy == 0, dy == ry - 1, dz == 0, dz == rz - 1};
 #pragma unroll
       for (int f = 0; f < 6; f++) {
         const T lw = wf ? wf[f * cellsf + cf] : ((cd >> f) & 1 ? T(1) : T(0));
@@ -292,20 +296,18 @@ __global__ void __launch_bounds__(CHUNK) k_compact_write(const uint8_t* flag, lo
 // ---------------------------------------------------------------- stencil helpers
 
 template <typename T>
-__device__ __forceinline__ T nsum(const T* x, int c, uint8_t cd, int n) {
-  const int nxy = n * n;
+__device__ __forceinline__ T nsum(const T* x, int c, uint8_t cd, int nx, int nxy) {
   T a = (cd & 1) ? x[c - 1] : T(0), b = (cd & 2) ? x[c + 1] : T(0);
-  T e = (cd & 4) ? x[c - n] : T(0), f = (cd & 8) ? x[c + n] : T(0);
+  T e = (cd & 4) ? x[c - nx] : T(0), f = (cd & 8) ? x[c + nx] : T(0);
   T g = (cd & 16) ? x[c - nxy] : T(0), h = (cd & 32) ? x[c + nxy] : T(0);
   return ((a + b) + (e + f)) + (g + h);
 }
 
 // Weighted neighbour sum of a coarse level (link weights w[f * cells + c]).
 template <typename T>
-__device__ __forceinline__ T wsum(const T* x, const T* w, int cells, int c, uint8_t cd, int n) {
-  const int nxy = n * n;
+__device__ __forceinline__ T wsum(const T* x, const T* w, int cells, int c, uint8_t cd, int nx, int nxy) {
   T a = (cd & 1) ? w[c] * x[c - 1] : T(0), b = (cd & 2) ? w[cells + c] * x[c + 1] : T(0);
-  T e = (cd & 4) ? w[2 * cells + c] * x[c - n] : T(0), f = (cd & 8) ? w[3 * cells + c] * x[c + n] : T(0);
+  T e = (cd & 4) ? w[2 * cells + c] * x[c - nx] : T(0), f = (cd & 8) ? w[3 * cells + c] * x[c + nx] : T(0);
   T g = (cd & 16) ? w[4 * cells + c] * x[c - nxy] : T(0), h = (cd & 32) ? w[5 * cells + c] * x[c + nxy] : T(0);
   return ((a + b) + (e + f)) + (g + h);
 }
@@ -313,12 +315,12 @@ __device__ __forceinline__ T wsum(const T* x, const T* w, int cells, int c, uint
 // Off-diagonal sum and diagonal of level (unit links and diagonal bytes when w is null).
 template <typename T>
 __device__ __forceinline__ void row_sum(const T* x, const uint8_t* diag, const T* w, const T* dg, int cells, int c,
-                                    uint8_t cd, int n, T& off, T& d) {
+                                        uint8_t cd, int nx, int nxy, T& off, T& d) {
   if (w) {
-    off = wsum(x, w, cells, c, cd, n);
+    off = wsum(x, w, cells, c, cd, nx, nxy);
     d = dg[c];
   } else {
-    off = nsum(x, c, cd, n);
+    off = nsum(x, c, cd, nx, nxy);
     d = T(diag[c]);
   }
 }
@@ -345,19 +347,19 @@ __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const u
   const int j = (tj << G.lty) + (row & (G.ty - 1));
   const int k = tk * G.tz + (row >> G.lty);
   const int i = (ti_ << G.ltx) + 2 * (u & ((1 << hx) - 1)) + ((color + j + k) & 1);
-  const int c = (s << G.lnc) + (((k << G.ln) + j) << G.ln) + i;
+  const int c = (s << G.lnc) + (((k << G.lny) + j) << G.lnx) + i;
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   T off = T(0), d;
   if (first) d = w ? dg[c] : T(diag[c]);
-  else row_sum(x, diag, w, dg, cells, c, cd, G.n, off, d);
+  else row_sum(x, diag, w, dg, cells, c, cd, G.nx, G.nx * G.ny, off, d);
   x[c] = (b[c] + off) / d;
 }
 
 // Coarse right-hand side: the sum of the unknown children's residuals b - A x (P^T r). The last
 // pre-smoothing half-sweep updated the black cells from their red neighbours, so a black residual is
-// zero up to rounding and only the four red children ((dx + dy + dz) even) are summed. Two tiles per
-// CTA, two coarse cells per thread.
+// zero up to rounding and only the red children ((i + j + k) even) are summed. Two tiles per CTA, two
+// coarse cells per thread.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* listc, const uint8_t* codef,
                                                      const uint8_t* diagf, const T* wf, const T* dgf, int cellsf,
@@ -367,22 +369,24 @@ __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* lis
   if (ti >= nact) return;
   const int gt = listc[ti];
   if (st[gt >> Gc.lnt].done) return;
-  const int nf = Gf.n;
+  const int rx = Gc.rx, ry = Gc.ry, rz = Gc.rz, nxf = Gf.nx, nxyf = Gf.nx * Gf.ny;
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     int s, i, j, k, c;
     tile_cell(Gc, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
     if (!(codec[c] & C_SELF)) continue;
-    const int base = (s << Gf.lnc) + ((2 * k) * nf + 2 * j) * nf + 2 * i;
-    const int kid[4] = {0, 1 + nf, 1 + nf * nf, nf + nf * nf};  // (0,0,0), (1,1,0), (1,0,1), (0,1,1)
+    const int fi = rx * i, fj = ry * j, fk = rz * k;
+    const int base = (s << Gf.lnc) + (fk * Gf.ny + fj) * nxf + fi;
     T acc = T(0);
 #pragma unroll
-    for (int q2 = 0; q2 < 4; q2++) {
-      const int cf = base + kid[q2];
+    for (int q2 = 0; q2 < 8; q2++) {
+      const int dx = q2 & 1, dy = (q2 >> 1) & 1, dz = q2 >> 2;
+      if (dx >= rx || dy >= ry || dz >= rz || ((fi + fj + fk + dx + dy + dz) & 1)) continue;
+      const int cf = base + dx + dy * nxf + dz * nxyf;
       const uint8_t cd = codef[cf];
       if (!(cd & C_SELF)) continue;
       T off, d;
-      row_sum(xf, diagf, wf, dgf, cellsf, cf, cd, nf, off, d);
+      row_sum(xf, diagf, wf, dgf, cellsf, cf, cd, nxf, nxyf, off, d);
       acc += bf[cf] - (d * xf[cf] - off);
     }
     bc[c] = acc;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* list
     int s, i, j, k, c;
     tile_cell(Gf, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
     if (!(codef[c] & C_SELF)) continue;
-    const int cc = (s << Gc.lnc) + (((k >> 1) * Gc.n + (j >> 1)) * Gc.n) + (i >> 1);
+    const int cc = (s << Gc.lnc) + ((k >> (Gc.rz - 1)) * Gc.ny + (j >> (Gc.ry - 1))) * Gc.nx + (i >> (Gc.rx - 1));
     if (codec[cc] & C_SELF) xf[c] += T(MG_OMEGA) * xc[cc];
   }
 }
@@ -416,8 +420,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(TG G, const uint8_t* code,
   __shared__ T sx[512];
   const int s = blockIdx.x;
   if (st[s].done) return;
-  const int n = G.n;  // 8
-  const int ncell = n * n * n;
+  const int nx = G.nx, nxy = G.nx * G.ny;
+  const int ncell = int(G.nc);  // at most 512
   const int t = threadIdx.x;
   const int c = (s << G.lnc) + t;
   uint8_t cd = 0;
@@ -429,7 +433,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(TG G, const uint8_t* code,
     bb = b[c];
 #pragma unroll
     for (int f = 0; f < 6; f++) w6[f] = w[f * cells + c];
-    const int i = t % n, j = (t / n) % n, k = t / (n * n);
+    const int i = t % nx, j = (t / nx) % G.ny, k = t / nxy;
     par = (i + j + k) & 1;
     sx[t] = T(0);
   }
@@ -438,9 +442,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(TG G, const uint8_t* code,
     T v = T(0);
     const bool act = t < ncell && (cd & C_SELF) && par == color;
     if (act) {
-      const int nxy = n * n;
       T a = (cd & 1) ? w6[0] * sx[t - 1] : T(0), b2 = (cd & 2) ? w6[1] * sx[t + 1] : T(0);
-      T e = (cd & 4) ? w6[2] * sx[t - n] : T(0), f = (cd & 8) ? w6[3] * sx[t + n] : T(0);
+      T e = (cd & 4) ? w6[2] * sx[t - nx] : T(0), f = (cd & 8) ? w6[3] * sx[t + nx] : T(0);
       T g = (cd & 16) ? w6[4] * sx[t - nxy] : T(0), h = (cd & 32) ? w6[5] * sx[t + nxy] : T(0);
       v = (bb + (((a + b2) + (e + f)) + (g + h))) / d;
     }
@@ -461,17 +464,19 @@ __global__ void __launch_bounds__(1024) k_mg_coarsest(TG G, const uint8_t* code,
 
 // ---------------------------------------------------------------- MIC(0) kernels (plane d = i + j + k)
 
+__device__ __forceinline__ int ilog2_dev(int v) { return 31 - __clz(v); }
+
 // Factor (solver3d.ts:883-900) with a(c, c + e) = -1 iff both cells are unknowns.
 template <typename T>
 __global__ void k_mic_factor(TG G, const uint8_t* code, const uint8_t* diag, T* pc, int d, int count) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = G.n;
-  if (t >= (count << (2 * G.ln))) return;
-  const int s = t >> (2 * G.ln), j = t & (n - 1), k = (t >> G.ln) & (n - 1);
+  const int nx = G.nx;
+  if (t >= (count << (G.lny + ilog2_dev(G.nz)))) return;
+  const int s = t >> (G.lny + ilog2_dev(G.nz)), j = t & (G.ny - 1), k = (t >> G.lny) & (G.nz - 1);
   const int i = d - j - k;
-  if (i < 1 || i > n - 2) return;
-  const int nxy = n * n;
-  const int c = (s << G.lnc) + ((k << G.ln) + j) * n + i;
+  if (i < 1 || i > nx - 2 || j < 1 || j > G.ny - 2 || k < 1 || k > G.nz - 2) return;
+  const int n = nx, nxy = nx * G.ny;
+  const int c = (s << G.lnc) + ((k << G.lny) + j) * nx + i;
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   const double tau = 0.97;
@@ -496,14 +501,14 @@ template <typename T>
 __global__ void k_mic_fwd(TG G, const uint8_t* code, const T* pc, const T* r, T* qv, int d, int count,
                           const Snap* st) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = G.n;
-  if (t >= (count << (2 * G.ln))) return;
-  const int s = t >> (2 * G.ln), j = t & (n - 1), k = (t >> G.ln) & (n - 1);
+  const int nx = G.nx;
+  if (t >= (count << (G.lny + ilog2_dev(G.nz)))) return;
+  const int s = t >> (G.lny + ilog2_dev(G.nz)), j = t & (G.ny - 1), k = (t >> G.lny) & (G.nz - 1);
   const int i = d - j - k;
-  if (i < 1 || i > n - 2) return;
+  if (i < 1 || i > nx - 2 || j < 1 || j > G.ny - 2 || k < 1 || k > G.nz - 2) return;
   if (st[s].done) return;
-  const int nxy = n * n;
-  const int c = (s << G.lnc) + ((k << G.ln) + j) * n + i;
+  const int n = nx, nxy = nx * G.ny;
+  const int c = (s << G.lnc) + ((k << G.lny) + j) * nx + i;
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   T v = r[c];
@@ -518,14 +523,14 @@ template <typename T>
 __global__ void k_mic_bwd(TG G, const uint8_t* code, const T* pc, const T* qv, T* z, int d, int count,
                           const Snap* st) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = G.n;
-  if (t >= (count << (2 * G.ln))) return;
-  const int s = t >> (2 * G.ln), j = t & (n - 1), k = (t >> G.ln) & (n - 1);
+  const int nx = G.nx;
+  if (t >= (count << (G.lny + ilog2_dev(G.nz)))) return;
+  const int s = t >> (G.lny + ilog2_dev(G.nz)), j = t & (G.ny - 1), k = (t >> G.lny) & (G.nz - 1);
   const int i = d - j - k;
-  if (i < 1 || i > n - 2) return;
+  if (i < 1 || i > nx - 2 || j < 1 || j > G.ny - 2 || k < 1 || k > G.nz - 2) return;
   if (st[s].done) return;
-  const int nxy = n * n;
-  const int c = (s << G.lnc) + ((k << G.ln) + j) * n + i;
+  const int n = nx, nxy = nx * G.ny;
+  const int c = (s << G.lnc) + ((k << G.lny) + j) * nx + i;
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   const T p = pc[c];
@@ -617,7 +622,7 @@ __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uin
   double v = 0;
   if (live) {
     const T beta = T(st[snap].beta);
-    const int n = G.n, nxy = n * n;
+    const int n = G.nx, nxy = G.nx * G.ny;
     auto pn = [&](int q) { return z[q] + beta * pold[q]; };
 #pragma unroll
     for (int q = 0; q < 2; q++) {
@@ -675,7 +680,7 @@ __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const ui
       tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
       const uint8_t cd = code[c];
       if (!(cd & C_SELF)) continue;
-      const double rt = double(b[c]) - (double(diag[c]) * x[c] - nsum(x, c, cd, G.n));
+      const double rt = double(b[c]) - (double(diag[c]) * x[c] - nsum(x, c, cd, G.nx, G.nx * G.ny));
       r[c] = T(rt);
       v = fmax(v, fabs(rt));
     }
@@ -788,7 +793,7 @@ namespace {
 
 template <typename T>
 struct PoissonT : PoissonImpl {
-  int n, count, method;
+  int count, method;
   int nlev = 0;
   Lvl<T> L[PMAXLEV];
   void* mem = nullptr;
@@ -807,14 +812,21 @@ struct PoissonT : PoissonImpl {
     if (pinned) cudaFreeHost(pinned);
   }
 
-  int init(int n_, int count_, int method_, char* err, size_t errlen) {
-    n = n_, count = count_, method = method_;
-    int m = n;
+  // last MIC(0) plane: i + j + k of the far interior corner
+  int dmax() const { return (L[0].G.nx - 2) + (L[0].G.ny - 2) + (L[0].G.nz - 2); }
+
+  int init(int nx, int ny, int nz, int count_, int method_, char* err, size_t errlen) {
+    count = count_, method = method_;
+    // levels: halve every axis longer than 8 until none is (semi-coarsening keeps thin boxes going)
+    int ex[3] = {nx, ny, nz}, rf[3] = {1, 1, 1};
     while (nlev < PMAXLEV) {
-      L[nlev].G = make_tg(m);
+      L[nlev].G = make_tg(ex[0], ex[1], ex[2], rf[0], rf[1], rf[2]);
       nlev++;
-      if (method != PL_POISSON_MG || m <= 8) break;
-      m /= 2;
+      if (method != PL_POISSON_MG || (ex[0] <= 8 && ex[1] <= 8 && ex[2] <= 8)) break;
+      for (int a = 0; a < 3; a++) {
+        rf[a] = ex[a] > 8 ? 2 : 1;
+        ex[a] /= rf[a];
+      }
     }
     std::vector<size_t> sizes;
     auto add = [&](size_t b) {
@@ -909,10 +921,10 @@ struct PoissonT : PoissonImpl {
     for (int l = 0; l < nlev; l++) L[l].nact = pinned[l];
     if (method == PL_POISSON_MIC0) {
       const TG& G = L[0].G;
-      const long long thr = (long long)count * G.n * G.n;
+      const long long thr = (long long)count * G.ny * G.nz;
       const unsigned blocks = unsigned((thr + 255) / 256);
       cudaMemsetAsync(pc, 0, size_t(count) * G.nc * sizeof(T), s0);
-      for (int d = 3; d <= 3 * (G.n - 2); d++) k_mic_factor<T><<<blocks, 256, 0, s0>>>(G, L[0].code, L[0].diag, pc, d, count);
+      for (int d = 3; d <= dmax(); d++) k_mic_factor<T><<<blocks, 256, 0, s0>>>(G, L[0].code, L[0].diag, pc, d, count);
     }
     return cudaGetLastError() == cudaSuccess ? PL_OK : PL_E_CUDA;
   }
@@ -921,10 +933,10 @@ struct PoissonT : PoissonImpl {
   void precondition(cudaStream_t s0) {
     if (method == PL_POISSON_MIC0) {
       const TG& G = L[0].G;
-      const long long thr = (long long)count * G.n * G.n;
+      const long long thr = (long long)count * G.ny * G.nz;
       const unsigned blocks = unsigned((thr + 255) / 256);
-      for (int d = 3; d <= 3 * (G.n - 2); d++) k_mic_fwd<T><<<blocks, 256, 0, s0>>>(G, L[0].code, pc, r, qv, d, count, st);
-      for (int d = 3 * (G.n - 2); d >= 3; d--) k_mic_bwd<T><<<blocks, 256, 0, s0>>>(G, L[0].code, pc, qv, z, d, count, st);
+      for (int d = 3; d <= dmax(); d++) k_mic_fwd<T><<<blocks, 256, 0, s0>>>(G, L[0].code, pc, r, qv, d, count, st);
+      for (int d = dmax(); d >= 3; d--) k_mic_bwd<T><<<blocks, 256, 0, s0>>>(G, L[0].code, pc, qv, z, d, count, st);
       return;
     }
     auto X = [&](int l) { return l == 0 ? z : L[l].x; };
@@ -948,7 +960,7 @@ struct PoissonT : PoissonImpl {
                                                              L[l + 1].b, st, L[l + 1].nact);
     }
     if (L[top].nact) {
-      if (top == 0 || L[top].G.n > 8) {  // no level small enough for one CTA: plain red-black sweeps
+      if (top == 0 || L[top].G.nc > 512) {  // no level small enough for one CTA: plain red-black sweeps
         for (int q = 0; q < COARSE_SWEEPS; q++) {
           smooth(top, 0, q == 0);
           smooth(top, 1, 0);
@@ -1255,15 +1267,16 @@ int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int t
   return PL_OK;
 }
 
-PoissonImpl* poisson_create(int n, int count, int method, int precision, char* err, size_t errlen, int* rc) {
+PoissonImpl* poisson_create(int nx, int ny, int nz, int count, int method, int precision, char* err, size_t errlen,
+                            int* rc) {
   PoissonImpl* h = nullptr;
   if (precision == PL_SOLVE_F64) {
     auto* q = new PoissonT<double>();
-    *rc = q->init(n, count, method, err, errlen);
+    *rc = q->init(nx, ny, nz, count, method, err, errlen);
     h = q;
   } else {
     auto* q = new PoissonT<float>();
-    *rc = q->init(n, count, method, err, errlen);
+    *rc = q->init(nx, ny, nz, count, method, err, errlen);
     h = q;
   }
   if (*rc) {

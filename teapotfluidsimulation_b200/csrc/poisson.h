@@ -11,7 +11,8 @@ struct PoissonImpl;
 
 int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int threads);
 int gauge_fix_one(int n, uint8_t* cell, float* b);
-PoissonImpl* poisson_create(int n, int count, int method, int precision, char* err, size_t errlen, int* rc);
+PoissonImpl* poisson_create(int nx, int ny, int nz, int count, int method, int precision, char* err, size_t errlen,
+                            int* rc);
 int poisson_solve(PoissonImpl* h, const uint8_t* cell, const float* b, double* x, double tol, int max_iter,
                   cudaStream_t st, int* iters, double* res, int* conv, char* err, size_t errlen);
 void poisson_destroy(PoissonImpl* h);

@@ -30,7 +30,7 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
+    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
     L.pl_poisson_gauge_fix.argtypes = [C.c_int32, C.c_int32, u8p, fp, C.POINTER(C.c_int32)]
     L.pl_poisson_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(P)]
+    L.pl_poisson_create_box.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                        C.POINTER(P)]
     L.pl_poisson_solve.argtypes = [P, P, P, P, C.c_double, C.c_int32, P, C.POINTER(C.c_int32), dp,
                                    C.POINTER(C.c_int32)]
     L.pl_poisson_device_bytes.argtypes = [P]
@@ -399,10 +401,12 @@ def poisson_gauge_fix(n: int, cell: np.ndarray, b: np.ndarray) -> np.ndarray:
 class PoissonBatch:
     """Batched dense-grid pressure solver (pl_poisson_create / pl_poisson_solve) on device buffers."""
 
-    def __init__(self, n: int, count: int, method: int, precision: int):
-        self.n, self.count = n, count
+    def __init__(self, n, count: int, method: int, precision: int):
+        """n: the cube's edge, or (nx, ny, nz) of a box (powers of two)."""
+        nx, ny, nz = (n, n, n) if isinstance(n, int) else tuple(n)
+        self.n, self.count, self.shape = nx, count, (nx, ny, nz)
         h = C.c_void_p()
-        _check(lib().pl_poisson_create(n, count, method, precision, C.byref(h)))
+        _check(lib().pl_poisson_create_box(nx, ny, nz, count, method, precision, C.byref(h)))
         self._h = h
 
     @property

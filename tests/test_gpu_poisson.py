@@ -9,6 +9,7 @@ import pytest
 import torch
 
 from poisson_util import FLUID, SOLID, AIR, apply_a
+from teapotfluidsimulation_b200 import abi
 
 pytestmark = pytest.mark.gpu
 
@@ -115,3 +116,41 @@ def test_empty_and_zero_rhs(engine):
     cell[1] = SOLID                           # no unknowns at all
     x, it, res, conv = solve(engine, cell, b, n, E.POISSON_MG, engine.abi.SOLVE_MIXED, 1e-6)
     assert it.tolist() == [0, 0] and conv.all() and (x == 0).all()
+
+
+def pour_box(oracle_mod, box, mm=10, steps=5):
+    """A pressure system of the reference pour (the oracle after a few substeps) in a SOLID-padded box:
+    the cells, and b = A q for the oracle's pressure q (so the exact solution is known)."""
+    sim = oracle_mod.OracleSim(abi.gentle_pour(mm, 1.0))
+    for _ in range(steps):
+        sim.step(-1)
+    nx, ny, nz = sim.nx, sim.ny, sim.nz
+    cell = sim.field(abi.FIELD_CELL).reshape(nz, ny, nx)
+    q = sim.field(abi.FIELD_PRESSURE).reshape(nz, ny, nx)
+    X, Y, Z = box
+    bc = np.full((Z, Y, X), SOLID, np.uint8)
+    bc[:nz, :ny, :nx] = cell
+    bq = np.zeros((Z, Y, X))
+    bq[:nz, :ny, :nx] = np.where(cell == FLUID, q, 0)
+    bc = bc.reshape(1, -1)
+    b = apply_a(bc[0], bq.reshape(-1), box).astype(np.float32)
+    return bc, b.reshape(1, -1)
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_box_of_a_pour_system(engine, oracle_mod, method):
+    E = engine.engine
+    box = (64, 64, 16)
+    cell, b = pour_box(oracle_mod, box)
+    E2 = engine.engine
+    dc, db = torch.from_numpy(cell).cuda(), torch.from_numpy(b).cuda()
+    dx = torch.zeros((1, int(np.prod(box))), dtype=torch.float64, device="cuda")
+    pb = E2.PoissonBatch(box, 1, method, engine.abi.SOLVE_F64)
+    it, res, conv = pb.solve(dc.data_ptr(), db.data_ptr(), dx.data_ptr(), 1e-10, 2000)
+    pb.destroy()
+    x = dx.cpu().numpy()[0]
+    q, oit, oconv, _ = oracle_mod.poisson_solve(cell[0], b[0].astype(np.float64), box, tol=1e-10)
+    assert conv[0] and oconv
+    assert np.abs(x - q).max() <= 1e-8 * np.abs(q).max()
+    if method == 0:
+        assert abs(int(it[0]) - oit) <= 1
