@@ -374,8 +374,9 @@ int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q,
  * unknowns. Snapshots are stored back to back, x fastest. */
 #define PL_POISSON_PIN 4
 enum pl_poisson_method {
-  PL_POISSON_MIC0 = 0, /* the reference's MIC(0) (solver3d.ts:883-900, 955-973), level-scheduled */
-  PL_POISSON_MG = 1    /* one V-cycle of 3D geometric multigrid (src/sim/multigrid.ts in 3D, RBGS) */
+  PL_POISSON_MIC0 = 0,   /* the reference's MIC(0) (solver3d.ts:883-900, 955-973), level-scheduled */
+  PL_POISSON_MG = 1,     /* one V-cycle of 3D geometric multigrid (src/sim/multigrid.ts in 3D, RBGS) */
+  PL_POISSON_LEARNED = 2 /* flexible CG with a pl_unet as preconditioner, MG fallback on a stall */
 };
 /* Synthetic workload on the host: snapshots first .. first+count-1 of n^3 cells (n a power of two in
  * [8, 512]): a solid cylinder wall (radius 60/128 n) and border, a liquid bottom slab (n/8) and 1-8
@@ -404,20 +405,22 @@ int pl_poisson_create_box(int32_t nx, int32_t ny, int32_t nz, int32_t count, int
  * arrays of count entries (any may be NULL). Synchronous. */
 int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double* x, double tol, int32_t max_iter,
                      void* stream, int32_t* iterations, double* residual, int32_t* converged);
+/* The network of PL_POISSON_LEARNED (the caller keeps it alive while the solver uses it). */
+typedef struct pl_unet pl_unet;
+int pl_poisson_set_unet(pl_poisson* h, pl_unet* u);
 /* Device bytes the solver holds. */
 size_t pl_poisson_device_bytes(const pl_poisson* h);
 void pl_poisson_destroy(pl_poisson* h);
 
 /* ------------------------------------------------------------------ learned preconditioner */
 
-/* A 3-level 3D convolutional U-Net (16/32/64 channels, 3^3 kernels, BF16 weights and activations,
+/* (pl_unet is declared with the Poisson batch above.) A 3-level 3D convolutional U-Net (16/32/64 channels, 3^3 kernels, BF16 weights and activations,
  * FP32 accumulation) that maps a residual r to an approximate correction z ~ A^-1 r on the liquid
  * cells of a box (no counterpart in the reference). Inputs: [r / max|r|, liquid mask, air mask];
  * output scaled by max|r| and zero off the liquid. Boxes are nx x ny x nz cells (multiples of 4), count
  * of them back to back, x fastest; cell u8 (PL_AIR / PL_FLUID / PL_SOLID), r, z, e f32, all device
  * buffers. Parameters are FP32 masters (per layer W[27][cin][cout] then the biases), trained by Adam
  * on the relative squared error sum_liquid (z - e)^2 / sum_liquid e^2, averaged over the boxes. */
-typedef struct pl_unet pl_unet;
 int pl_unet_create(uint32_t seed, pl_unet** out);
 int32_t pl_unet_num_params(const pl_unet* u);
 int pl_unet_get_params(pl_unet* u, float* host);

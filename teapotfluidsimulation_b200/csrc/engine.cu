@@ -907,6 +907,11 @@ int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q,
 
 // ------------------------------------------------------------------ Poisson batch
 
+struct pl_unet {
+  pl::UNetImpl* impl;
+  int device;
+};
+
 struct pl_poisson {
   pl::PoissonImpl* impl;
   int n, count, device;
@@ -939,7 +944,7 @@ int pl_poisson_create_box(int32_t nx, int32_t ny, int32_t nz, int32_t count, int
   if (!pow2(nx) || !pow2(ny) || !pow2(nz) || count < 1)
     return fail(PL_E_ARG, "pl_poisson_create: box extents must be powers of two in [8, 512] and count >= 1 "
                 "(%dx%dx%d, count=%d)", nx, ny, nz, count);
-  if (method != PL_POISSON_MIC0 && method != PL_POISSON_MG)
+  if (method != PL_POISSON_MIC0 && method != PL_POISSON_MG && method != PL_POISSON_LEARNED)
     return fail(PL_E_ARG, "pl_poisson_create: unknown method %d", method);
   if (precision != PL_SOLVE_F64 && precision != PL_SOLVE_MIXED)
     return fail(PL_E_ARG, "pl_poisson_create: unknown precision %d", precision);
@@ -971,6 +976,12 @@ int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double*
   return PL_OK;
 }
 
+int pl_poisson_set_unet(pl_poisson* h, pl_unet* u) {
+  if (!h || !u) return fail(PL_E_ARG, "pl_poisson_set_unet: null argument");
+  pl::poisson_set_unet(h->impl, u->impl);
+  return PL_OK;
+}
+
 size_t pl_poisson_device_bytes(const pl_poisson* h) { return h ? pl::poisson_bytes(h->impl) : 0; }
 
 void pl_poisson_destroy(pl_poisson* h) {
@@ -982,10 +993,6 @@ void pl_poisson_destroy(pl_poisson* h) {
 
 // ------------------------------------------------------------------ learned preconditioner
 
-struct pl_unet {
-  pl::UNetImpl* impl;
-  int device;
-};
 
 int pl_unet_create(uint32_t seed, pl_unet** out) {
   if (!out) return fail(PL_E_ARG, "pl_unet_create: null argument");

@@ -32,6 +32,11 @@
 //    internal links. Two sweeps (red, black) before and (black, red) after the coarse correction,
 //    which is over-relaxed by 1.5, and a palindromic sweep sequence on the coarsest level (8^3 per
 //    snapshot, one CTA): the V-cycle is a symmetric operator, so CG stays valid.
+//  - LEARNED: flexible CG (Polak-Ribiere beta) with the U-Net of unet.cu as the preconditioner
+//    (z = the network's output for r), and the multigrid above as the fallback: a snapshot whose
+//    max-norm residual falls less than 2x over 5 iterations (or that reaches 200 network iterations)
+//    switches to multigrid and restarts CG from its FP64 true residual; every snapshot still ends on
+//    the same max-norm rule.
 //  - MIC0: the reference's MIC(0) factor and triangular sweeps (solver3d.ts:883-900, 955-973). A
 //    cell depends only on its -x, -y, -z neighbours, so the planes i + j + k = d, processed in
 //    increasing (forward) or decreasing (backward) order, give exactly the sequential result; one
@@ -45,6 +50,7 @@
 
 #include "common.cuh"
 #include "poisson.h"
+#include "unet.h"
 
 namespace pl {
 
@@ -118,7 +124,14 @@ struct Snap {
   double bnorm, target;
   double rz, rz_old, alpha, beta, res;
   int it, done, converged, check, restarts, fresh;
+  // learned preconditioning: 0 = the network, 1 = multigrid (after a stall); max |r| of the last
+  // iterations (ring) for the stall test; iterations taken with the network
+  int pre, learned_it;
+  double hist[8];
 };
+
+constexpr int STALL_SPAN = 5;      // the network stalls when max|r| fell less than 2x over this many iterations
+constexpr int LEARNED_CAP = 200;   // ... or after this many iterations with it
 
 template <typename T>
 struct Lvl {
@@ -596,20 +609,39 @@ __global__ void __launch_bounds__(PT) k_pcg_init(TG G, const int* list, const ui
 }
 
 // Partial z.r per tile.
+// Partial z.r per tile; with r_old (flexible CG) also z.r_old into part2.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint8_t* code, const T* r, const T* z,
-                                               double* part, const Snap* st, int nact) {
+                                               const T* rold, double* part, double* part2, const Snap* st, int nact) {
   PCG_TILE_PROLOGUE
-  double v = 0;
+  double v = 0, v2 = 0;
   if (live) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       int s, i, j, k, c;
       tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
-      if (code[c] & C_SELF) v += double(z[c]) * double(r[c]);
+      if (code[c] & C_SELF) {
+        v += double(z[c]) * double(r[c]);
+        if (rold) v2 += double(z[c]) * double(rold[c]);
+      }
     }
   }
   half_store(v, live ? &part[gt] : nullptr, false);
+  if (rold) half_store(v2, live ? &part2[gt] : nullptr, false);
+}
+
+// Learned preconditioning: z = the network's output zn on the snapshots that still use it.
+template <typename T>
+__global__ void __launch_bounds__(PT) k_select_pre(TG G, const int* list, const uint8_t* code, const float* zn, T* z,
+                                                   const Snap* st, int nact) {
+  PCG_TILE_PROLOGUE
+  if (!live || st[snap].pre) return;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    int s, i, j, k, c;
+    tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
+    if (code[c] & C_SELF) z[c] = T(zn[c]);
+  }
 }
 
 // p = z + beta p_old into p_new and A p_new (neighbours' new p formed on the fly from z and p_old, which
@@ -646,7 +678,7 @@ __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uin
 // x += alpha p, r -= alpha Ap; max |r| per tile.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const uint8_t* code, double* x, const T* p,
-                                                   T* r, const T* ap, double* part, const Snap* st, int nact) {
+                                                   T* r, const T* ap, T* rold, double* part, const Snap* st, int nact) {
   PCG_TILE_PROLOGUE
   double v = 0;
   if (live) {
@@ -657,6 +689,7 @@ __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const 
       tile_cell(G, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
       if (!(code[c] & C_SELF)) continue;
       x[c] += a * double(p[c]);
+      if (rold) rold[c] = r[c];
       const T rv = r[c] - T(a) * ap[c];
       r[c] = rv;
       v = fmax(v, fabs(double(rv)));
@@ -691,8 +724,8 @@ __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const ui
 // Per-snapshot scalar steps from the per-tile partials (summed or maximised in tile order: inactive
 // tiles hold 0). phase 0: after init (max|b|: bnorm, target); 1: after z.r (beta); 2: after p.Ap
 // (alpha, breakdown); 3: after the update (max|r|: convergence, check); 4: after a true residual.
-__global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* part, long long ntile, Snap* st,
-                                                      double tol, int max_iter) {
+__global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* part, const double* part2,
+                                                      long long ntile, Snap* st, double tol, int max_iter, int learned) {
   const int s = blockIdx.x;
   Snap& S = st[s];
   __shared__ double sw[RED_T / 32];
@@ -715,9 +748,14 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
   double m = 0;
   for (int w = 0; w < RED_T / 32; w++) m = is_max ? fmax(m, sw[w]) : m + sw[w];
   if (phase == 1) {
+    double m2 = 0;  // z . r_old (flexible CG): one thread sums the tile partials in tile order
+    if (learned && !S.fresh)
+      for (long long t = 0; t < ntile; t++) m2 += part2[(long long)s * ntile + t];
     S.rz_old = S.rz;
     S.rz = m;
-    S.beta = S.fresh ? 0.0 : m / S.rz_old;
+    // Polak-Ribiere beta (z.(r - r_old) / z_old.r_old) keeps CG valid for a preconditioner that changes
+    // from one iteration to the next (the network is not a fixed symmetric operator)
+    S.beta = S.fresh ? 0.0 : (learned ? (m - m2) / S.rz_old : m / S.rz_old);
     S.fresh = 0;
     return;
   }
@@ -739,6 +777,9 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
     S.check = 0;
     S.restarts = 0;
     S.converged = 0;
+    S.pre = learned ? 0 : 1;
+    S.learned_it = 0;
+    for (int q = 0; q < 8; q++) S.hist[q] = m;
     S.done = (m < 1e-14) ? 1 : 0;  // solver3d.ts:901
     if (S.done) S.converged = 1;
     return;
@@ -746,6 +787,15 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
   if (phase == 3) {
     S.it++;
     S.res = m;
+    if (!S.pre) {
+      S.learned_it++;
+      const double before = S.hist[(S.it - STALL_SPAN) & 7];
+      if ((S.learned_it > STALL_SPAN && m > 0.5 * before) || S.learned_it >= LEARNED_CAP) {
+        S.pre = 1;    // the network stalls: multigrid from here on, CG restarted from the true residual
+        S.check = 1;
+      }
+    }
+    S.hist[S.it & 7] = m;
     if (m <= S.target) {
       S.check = 1;  // confirm with the true residual
     } else if (S.it >= max_iter) {
@@ -784,6 +834,7 @@ __global__ void k_pcg_alldone(const Snap* st, int count, int* out) {
 
 struct PoissonImpl {
   virtual ~PoissonImpl() {}
+  UNetImpl* net = nullptr;  // learned preconditioning (PL_POISSON_LEARNED), owned by the caller
   virtual int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t st,
                     int* iters, double* res, int* conv, char* err, size_t errlen) = 0;
   size_t bytes = 0;
@@ -798,7 +849,10 @@ struct PoissonT : PoissonImpl {
   Lvl<T> L[PMAXLEV];
   void* mem = nullptr;
   T *r = nullptr, *z = nullptr, *p = nullptr, *p1 = nullptr, *ap = nullptr, *pc = nullptr, *qv = nullptr;
-  double* part = nullptr;
+  T* rold = nullptr;     // learned: r of the previous iteration (flexible beta)
+  float* zn = nullptr;   // learned: the network's output
+  const uint8_t* cell_in = nullptr;
+  double *part = nullptr, *part2 = nullptr;
   Snap* st = nullptr;
   int* dcnt = nullptr;  // [PMAXLEV] active tile counters, [PMAXLEV] all-done flag
   int* chunk = nullptr;  // per-chunk counts / offsets of the list compaction
@@ -812,6 +866,8 @@ struct PoissonT : PoissonImpl {
     if (pinned) cudaFreeHost(pinned);
   }
 
+  bool learned() const { return method == PL_POISSON_LEARNED; }
+
   // last MIC(0) plane: i + j + k of the far interior corner
   int dmax() const { return (L[0].G.nx - 2) + (L[0].G.ny - 2) + (L[0].G.nz - 2); }
 
@@ -822,7 +878,7 @@ struct PoissonT : PoissonImpl {
     while (nlev < PMAXLEV) {
       L[nlev].G = make_tg(ex[0], ex[1], ex[2], rf[0], rf[1], rf[2]);
       nlev++;
-      if (method != PL_POISSON_MG || (ex[0] <= 8 && ex[1] <= 8 && ex[2] <= 8)) break;
+      if (method == PL_POISSON_MIC0 || (ex[0] <= 8 && ex[1] <= 8 && ex[2] <= 8)) break;
       for (int a = 0; a < 3; a++) {
         rf[a] = ex[a] > 8 ? 2 : 1;
         ex[a] /= rf[a];
@@ -852,6 +908,9 @@ struct PoissonT : PoissonImpl {
     const size_t i_pc = method == PL_POISSON_MIC0 ? add(C0 * sizeof(T)) : 0;
     const size_t i_qv = method == PL_POISSON_MIC0 ? add(C0 * sizeof(T)) : 0;
     const size_t i_part = add(size_t(count) * L[0].G.ntile * 8);
+    const size_t i_part2 = add(size_t(count) * L[0].G.ntile * 8);
+    const size_t i_rold = learned() ? add(C0 * sizeof(T)) : 0;
+    const size_t i_zn = learned() ? add(C0 * 4) : 0;
     const size_t i_st = add(size_t(count) * sizeof(Snap));
     const size_t i_cnt = add(2 * PMAXLEV * 4);
     const size_t i_chunk = add(size_t((size_t(count) * L[0].G.ntile + CHUNK - 1) / CHUNK) * 4);
@@ -884,6 +943,9 @@ struct PoissonT : PoissonImpl {
     pc = method == PL_POISSON_MIC0 ? (T*)at[i_pc] : nullptr;
     qv = method == PL_POISSON_MIC0 ? (T*)at[i_qv] : nullptr;
     part = (double*)at[i_part];
+    part2 = (double*)at[i_part2];
+    rold = learned() ? (T*)at[i_rold] : nullptr;
+    zn = learned() ? (float*)at[i_zn] : nullptr;
     st = (Snap*)at[i_st];
     dcnt = (int*)at[i_cnt];
     chunk = (int*)at[i_chunk];
@@ -929,8 +991,17 @@ struct PoissonT : PoissonImpl {
     return cudaGetLastError() == cudaSuccess ? PL_OK : PL_E_CUDA;
   }
 
-  // z = M r
+  // z = M r (learned: the network's z on the snapshots that have not fallen back to multigrid)
   void precondition(cudaStream_t s0) {
+    mg_or_mic0(s0);
+    if (!learned()) return;
+    char err[128];
+    const TG& G = L[0].G;
+    unet_apply(net, cell_in, reinterpret_cast<const float*>(r), zn, G.nx, G.ny, G.nz, count, s0, err, sizeof err);
+    k_select_pre<T><<<grid2(L[0].nact), PT, 0, s0>>>(G, L[0].list, L[0].code, zn, z, st, L[0].nact);
+  }
+
+  void mg_or_mic0(cudaStream_t s0) {
     if (method == PL_POISSON_MIC0) {
       const TG& G = L[0].G;
       const long long thr = (long long)count * G.ny * G.nz;
@@ -992,14 +1063,14 @@ struct PoissonT : PoissonImpl {
     const TG& G = L[0].G;
     const int na = L[0].nact;
     precondition(s0);
-    k_pcg_rz<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, G.ntile, st, tol, max_iter);
+    k_pcg_rz<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, rold, part, part2, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, part2, G.ntile, st, tol, max_iter, learned());
     k_pcg_pap<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, G.ntile, st, tol, max_iter);
-    k_pcg_update<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, G.ntile, st, tol, max_iter);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, part2, G.ntile, st, tol, max_iter, learned());
+    k_pcg_update<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, rold, part, st, na);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, part2, G.ntile, st, tol, max_iter, learned());
     k_pcg_true<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, G.ntile, st, tol, max_iter);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, part2, G.ntile, st, tol, max_iter, learned());
   }
 
   int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t s0, int* iters,
@@ -1009,13 +1080,23 @@ struct PoissonT : PoissonImpl {
       snprintf(err, errlen, "pl_poisson_solve: set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
       return rc;
     }
+    cell_in = cell;
+    if (learned()) {
+      if (!net) {
+        snprintf(err, errlen, "pl_poisson_solve: the learned method needs a network (pl_poisson_set_unet)");
+        return PL_E_STATE;
+      }
+      rc = unet_prepare(net, L[0].G.nx, L[0].G.ny, L[0].G.nz, count, err, errlen);  // before the capture
+      if (rc) return rc;
+      cudaMemsetAsync(rold, 0, size_t(count) * L[0].G.nc * sizeof(T), s0);
+    }
     const TG& G = L[0].G;
     const int na = L[0].nact;
     cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);  // inactive tiles' partials stay 0
     cudaMemsetAsync(x, 0, size_t(count) * G.nc * 8, s0);
     if (na > 0) k_pcg_init<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, b, r, x, p, part, st, na);
     cudaMemsetAsync(p1, 0, size_t(count) * G.nc * sizeof(T), s0);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, G.ntile, st, tol, max_iter);
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, part2, G.ntile, st, tol, max_iter, learned());
     if (na > 0) {
       // the iteration as a CUDA graph (one launch per iteration), checked for completion in batches
       if (iter_graph) {
@@ -1270,6 +1351,11 @@ int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int t
 PoissonImpl* poisson_create(int nx, int ny, int nz, int count, int method, int precision, char* err, size_t errlen,
                             int* rc) {
   PoissonImpl* h = nullptr;
+  if (method == PL_POISSON_LEARNED && precision != PL_SOLVE_MIXED) {
+    snprintf(err, errlen, "pl_poisson_create: the learned method runs with FP32 vectors (PL_SOLVE_MIXED)");
+    *rc = PL_E_ARG;
+    return nullptr;
+  }
   if (precision == PL_SOLVE_F64) {
     auto* q = new PoissonT<double>();
     *rc = q->init(nx, ny, nz, count, method, err, errlen);
@@ -1292,6 +1378,8 @@ int poisson_solve(PoissonImpl* h, const uint8_t* cell, const float* b, double* x
 }
 
 void poisson_destroy(PoissonImpl* h) { delete h; }
+
+void poisson_set_unet(PoissonImpl* h, UNetImpl* u) { h->net = u; }
 
 size_t poisson_bytes(const PoissonImpl* h) { return h ? h->bytes : 0; }
 

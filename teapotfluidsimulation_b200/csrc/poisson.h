@@ -8,6 +8,7 @@
 namespace pl {
 
 struct PoissonImpl;
+struct UNetImpl;
 
 int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int threads);
 int gauge_fix_one(int n, uint8_t* cell, float* b);
@@ -16,6 +17,7 @@ PoissonImpl* poisson_create(int nx, int ny, int nz, int count, int method, int p
 int poisson_solve(PoissonImpl* h, const uint8_t* cell, const float* b, double* x, double tol, int max_iter,
                   cudaStream_t st, int* iters, double* res, int* conv, char* err, size_t errlen);
 void poisson_destroy(PoissonImpl* h);
+void poisson_set_unet(PoissonImpl* h, UNetImpl* u);
 size_t poisson_bytes(const PoissonImpl* h);
 
 }  // namespace pl

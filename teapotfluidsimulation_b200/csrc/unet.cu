@@ -725,6 +725,11 @@ int unet_set_params(UNetImpl* u, const float* host) {
                                                                                                    : PL_E_CUDA;
 }
 
+int unet_prepare(UNetImpl* u, int X, int Y, int Z, int count, char* err, size_t errlen) {
+  int rc = check_box(X, Y, Z, count, err, errlen);
+  return rc ? rc : u->workspace(X, Y, Z, count, err, errlen);
+}
+
 int unet_apply(UNetImpl* u, const uint8_t* cell, const float* r, float* z, int X, int Y, int Z, int count,
                cudaStream_t st, char* err, size_t errlen) {
   int rc = check_box(X, Y, Z, count, err, errlen);

@@ -14,6 +14,7 @@ void unet_destroy(UNetImpl* u);
 int unet_nparams(const UNetImpl* u);
 int unet_get_params(UNetImpl* u, float* host);
 int unet_set_params(UNetImpl* u, const float* host);
+int unet_prepare(UNetImpl* u, int X, int Y, int Z, int count, char* err, size_t errlen);
 int unet_apply(UNetImpl* u, const uint8_t* cell, const float* r, float* z, int X, int Y, int Z, int count,
                cudaStream_t st, char* err, size_t errlen);
 int unet_gradient(UNetImpl* u, const uint8_t* cell, const float* r, const float* e, int X, int Y, int Z, int count,

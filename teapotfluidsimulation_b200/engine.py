@@ -30,7 +30,7 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
+    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -113,6 +113,7 @@ def lib() -> C.CDLL:
                                         C.POINTER(P)]
     L.pl_poisson_solve.argtypes = [P, P, P, P, C.c_double, C.c_int32, P, C.POINTER(C.c_int32), dp,
                                    C.POINTER(C.c_int32)]
+    L.pl_poisson_set_unet.argtypes = [P, P]
     L.pl_poisson_device_bytes.argtypes = [P]
     L.pl_poisson_device_bytes.restype = C.c_size_t
     L.pl_poisson_destroy.argtypes = [P]
@@ -378,6 +379,7 @@ def pcg_solve_device_noalloc(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny:
 
 POISSON_MIC0 = 0
 POISSON_MG = 1
+POISSON_LEARNED = 2
 POISSON_PIN = 4
 
 
