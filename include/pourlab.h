@@ -410,6 +410,13 @@ typedef struct pl_unet pl_unet;
 int pl_poisson_set_unet(pl_poisson* h, pl_unet* u);
 /* Device bytes the solver holds. */
 size_t pl_poisson_device_bytes(const pl_poisson* h);
+/* Convergence record of one snapshot of the last pl_poisson_solve: the recurrence's max-norm residual
+ * after each of its first PL_POISSON_HISTORY iterations (up to capacity entries written, recorded =
+ * how many exist) and, for PL_POISSON_LEARNED, the iterations preconditioned by the network before any
+ * fall-back to multigrid. (No counterpart in the reference; Pcg3D.solve returns only the totals.) */
+#define PL_POISSON_HISTORY 64
+int pl_poisson_history(const pl_poisson* h, int32_t snapshot, double* max_residual, int32_t capacity,
+                       int32_t* recorded, int32_t* learned_iterations);
 void pl_poisson_destroy(pl_poisson* h);
 
 /* ------------------------------------------------------------------ learned preconditioner */
@@ -422,6 +429,11 @@ void pl_poisson_destroy(pl_poisson* h);
  * buffers. Parameters are FP32 masters (per layer W[27][cin][cout] then the biases), trained by Adam
  * on the relative squared error sum_liquid (z - e)^2 / sum_liquid e^2, averaged over the boxes. */
 int pl_unet_create(uint32_t seed, pl_unet** out);
+/* Training loss: PL_UNET_LOSS_L2 (the default above) or PL_UNET_LOSS_ENERGY, the error in the operator's
+ * energy norm, (z - e).A(z - e) / e.Ae per box (unknowns: liquid cells off the box border), the norm in
+ * which a preconditioner's quality decides CG's convergence. */
+enum pl_unet_loss { PL_UNET_LOSS_L2 = 0, PL_UNET_LOSS_ENERGY = 1 };
+int pl_unet_set_loss(pl_unet* u, int32_t kind);
 int32_t pl_unet_num_params(const pl_unet* u);
 int pl_unet_get_params(pl_unet* u, float* host);
 int pl_unet_set_params(pl_unet* u, const float* host); /* also resets the Adam moments */

@@ -984,6 +984,14 @@ int pl_poisson_set_unet(pl_poisson* h, pl_unet* u) {
 
 size_t pl_poisson_device_bytes(const pl_poisson* h) { return h ? pl::poisson_bytes(h->impl) : 0; }
 
+int pl_poisson_history(const pl_poisson* h, int32_t snapshot, double* max_residual, int32_t capacity,
+                       int32_t* recorded, int32_t* learned_iterations) {
+  if (!h || (capacity > 0 && !max_residual)) return fail(PL_E_ARG, "pl_poisson_history: null argument");
+  if (pl::poisson_history(h->impl, snapshot, max_residual, capacity, recorded, learned_iterations))
+    return fail(PL_E_ARG, "pl_poisson_history: snapshot %d out of range or no solve yet", snapshot);
+  return PL_OK;
+}
+
 void pl_poisson_destroy(pl_poisson* h) {
   if (!h) return;
   cudaSetDevice(h->device);
@@ -1004,6 +1012,13 @@ int pl_unet_create(uint32_t seed, pl_unet** out) {
   pl_unet* u = new pl_unet{impl, 0};
   cudaGetDevice(&u->device);
   *out = u;
+  return PL_OK;
+}
+
+int pl_unet_set_loss(pl_unet* u, int32_t kind) {
+  if (!u) return fail(PL_E_ARG, "pl_unet_set_loss: null argument");
+  if (kind != PL_UNET_LOSS_L2 && kind != PL_UNET_LOSS_ENERGY) return fail(PL_E_ARG, "pl_unet_set_loss: kind %d", kind);
+  pl::unet_set_loss(u->impl, kind);
   return PL_OK;
 }
 

@@ -128,6 +128,7 @@ struct Snap {
   // iterations (ring) for the stall test; iterations taken with the network
   int pre, learned_it;
   double hist[8];
+  double rh[PL_POISSON_HISTORY];  // max |r| after iteration k + 1 (the first PL_POISSON_HISTORY iterations)
 };
 
 constexpr int STALL_SPAN = 5;      // the network stalls when max|r| fell less than 2x over this many iterations
@@ -787,6 +788,7 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
   if (phase == 3) {
     S.it++;
     S.res = m;
+    if (S.it <= PL_POISSON_HISTORY) S.rh[S.it - 1] = m;
     if (!S.pre) {
       S.learned_it++;
       const double before = S.hist[(S.it - STALL_SPAN) & 7];
@@ -838,6 +840,7 @@ struct PoissonImpl {
   virtual int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t st,
                     int* iters, double* res, int* conv, char* err, size_t errlen) = 0;
   size_t bytes = 0;
+  std::vector<Snap> last;  // per-snapshot state at the end of the last solve
 };
 
 namespace {
@@ -999,6 +1002,14 @@ struct PoissonT : PoissonImpl {
     const TG& G = L[0].G;
     unet_apply(net, cell_in, reinterpret_cast<const float*>(r), zn, G.nx, G.ny, G.nz, count, s0, err, sizeof err);
     k_select_pre<T><<<grid2(L[0].nact), PT, 0, s0>>>(G, L[0].list, L[0].code, zn, z, st, L[0].nact);
+    // the network's correction, then red-black Gauss-Seidel sweeps from it: the network carries the
+    // smooth part of the error, the sweeps the rough part (on a fallen-back snapshot they follow the
+    // V-cycle's own post-smoothing)
+    for (int q = 0; q < MG_NU; q++)
+      for (int color = 0; color < 2; color++)
+        k_mg_smooth<T><<<unsigned((L[0].nact + 1) / 2), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, L[0].w,
+                                                                     L[0].dg, int(count * G.nc), z, r, color, 0, st,
+                                                                     L[0].nact);
   }
 
   void mg_or_mic0(cudaStream_t s0) {
@@ -1145,6 +1156,7 @@ struct PoissonT : PoissonImpl {
       if (res) res[s] = hs[s].res;
       if (conv) conv[s] = hs[s].converged;
     }
+    last = std::move(hs);
     return PL_OK;
   }
 };
@@ -1382,5 +1394,15 @@ void poisson_destroy(PoissonImpl* h) { delete h; }
 void poisson_set_unet(PoissonImpl* h, UNetImpl* u) { h->net = u; }
 
 size_t poisson_bytes(const PoissonImpl* h) { return h ? h->bytes : 0; }
+
+int poisson_history(const PoissonImpl* h, int snapshot, double* out, int capacity, int* recorded, int* learned_it) {
+  if (snapshot < 0 || snapshot >= (int)h->last.size()) return PL_E_ARG;
+  const Snap& S = h->last[snapshot];
+  const int n = std::min(S.it, PL_POISSON_HISTORY);
+  for (int k = 0; k < std::min(n, capacity); k++) out[k] = S.rh[k];
+  if (recorded) *recorded = n;
+  if (learned_it) *learned_it = S.learned_it;
+  return PL_OK;
+}
 
 }  // namespace pl

@@ -19,5 +19,6 @@ int poisson_solve(PoissonImpl* h, const uint8_t* cell, const float* b, double* x
 void poisson_destroy(PoissonImpl* h);
 void poisson_set_unet(PoissonImpl* h, UNetImpl* u);
 size_t poisson_bytes(const PoissonImpl* h);
+int poisson_history(const PoissonImpl* h, int snapshot, double* out, int capacity, int* recorded, int* learned_it);
 
 }  // namespace pl

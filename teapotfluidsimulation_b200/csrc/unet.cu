@@ -417,6 +417,77 @@ __global__ void k_loss(Box B, const uint8_t* cell, const float* o, const float* 
   }
 }
 
+// An unknown of the pressure operator: a liquid cell off the box border.
+__device__ __forceinline__ bool is_unknown(const Box& B, const uint8_t* cell, int v, int x, int y, int z) {
+  return (cell[v] & 3) == FLUID && x > 0 && y > 0 && z > 0 && x < B.X - 1 && y < B.Y - 1 && z < B.Z - 1;
+}
+
+// Energy-norm loss terms, one block per box: d = s o - e on the unknowns, A d and A e with the 7-point
+// operator (diagonal: the non-SOLID neighbours, +1 on PL_POISSON_PIN cells; -1 between neighbouring
+// unknowns); writes A d, the energy e.Ae and the box's loss term d.Ad / (e.Ae count).
+__global__ void k_energy_terms(Box B, const uint8_t* cell, const float* o, const float* e, const float* scale,
+                               float* ad, float* energy, float* loss_part) {
+  const int s = blockIdx.x;
+  const int per = B.cells(), XY = B.X * B.Y;
+  const float sc = scale[s];
+  double dad = 0, eae = 0;
+  for (int c = threadIdx.x; c < per; c += blockDim.x) {
+    const int v = s * per + c;
+    const int x = c % B.X, y = (c / B.X) % B.Y, z = c / XY;
+    if (!is_unknown(B, cell, v, x, y, z)) {
+      ad[v] = 0.f;
+      continue;
+    }
+    const int nb6[6] = {v - 1, v + 1, v - B.X, v + B.X, v - XY, v + XY};
+    const int nx6[6] = {x - 1, x + 1, x, x, x, x}, ny6[6] = {y, y, y - 1, y + 1, y, y},
+              nz6[6] = {z, z, z, z, z - 1, z + 1};
+    const float dv = sc * o[(size_t)v * 16] - e[v];
+    float diag = (cell[v] & 4) ? 1.f : 0.f;
+    float sd = 0.f, se = 0.f;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int w = nb6[q];
+      if ((cell[w] & 3) != SOLID) diag += 1.f;
+      if (is_unknown(B, cell, w, nx6[q], ny6[q], nz6[q])) {
+        sd += sc * o[(size_t)w * 16] - e[w];
+        se += e[w];
+      }
+    }
+    const float a_d = diag * dv - sd, a_e = diag * e[v] - se;
+    ad[v] = a_d;
+    dad += double(dv) * a_d;
+    eae += double(e[v]) * a_e;
+  }
+  __shared__ double sh[2][256];
+  sh[0][threadIdx.x] = dad;
+  sh[1][threadIdx.x] = eae;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int q = 0; q < (int)blockDim.x; q++) {
+      a += sh[0][q];
+      b += sh[1][q];
+    }
+    const float en = b > 0 ? float(b) : 1.f;
+    energy[s] = en;
+    loss_part[s] = float(a) / (en * B.count);
+  }
+}
+
+// Gradient of the energy-norm loss with respect to o[v][0]: 2 s (A d)_v / (e.Ae count) (A is symmetric).
+__global__ void k_energy_grad(Box B, const float* ad, const float* scale, const float* energy, bf16* dout) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= B.total()) return;
+  const int s = v / B.cells();
+  bf16 ch[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) ch[q] = __float2bfloat16(0.f);
+  ch[0] = __float2bfloat16(2.f * scale[s] * ad[v] / (energy[s] * B.count));
+  uint4* dst = reinterpret_cast<uint4*>(dout + (size_t)v * 16);
+  dst[0] = *reinterpret_cast<uint4*>(&ch[0]);
+  dst[1] = *reinterpret_cast<uint4*>(&ch[8]);
+}
+
 __global__ void k_sum(const float* part, int n, float* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   float a = 0.f;
@@ -466,8 +537,9 @@ struct UNetImpl {
   size_t ws_bytes = 0;
   bf16 *x0, *a0, *s1, *p1, *a2, *s2, *p2, *a4, *a5, *c2, *a6, *a7, *c1, *a8, *a9;  // forward
   bf16 *d_o, *d_a9, *d_a8, *d_c1, *d_a7, *d_a6, *d_c2, *d_a5, *d_a4, *d_p2, *d_s2, *d_a2, *d_p1, *d_s1, *d_a0;
-  float *o, *scale, *energy, *part, *loss_part, *loss;
+  float *o, *scale, *energy, *part, *loss_part, *loss, *ad;
   int nchunk = 0, nloss = 0;
+  int loss_kind = 0;  // PL_UNET_LOSS_L2 or PL_UNET_LOSS_ENERGY
 
   ~UNetImpl() {
     if (wmem) cudaFree(wmem);
@@ -547,7 +619,8 @@ struct UNetImpl {
         n2 * 16, n1 * 16, n1 * 16};                                                              // gradients
     size_t bytes = 0;
     for (size_t s : sz) bytes += ((s * 2 + 255) & ~size_t(255));
-    const size_t fbytes = n1 * 16 * 4 + 2 * size_t(count) * 4 + size_t(nchunk) * maxw * 4 + size_t(nloss) * 4 + 1024;
+    const size_t fbytes = n1 * 16 * 4 + 2 * size_t(count) * 4 + size_t(nchunk) * maxw * 4 + size_t(nloss) * 4 + 1024 +
+                          n1 * 4 + 256;
     if (cudaMalloc(&ws, bytes + fbytes + 4096) != cudaSuccess) {
       ws = nullptr;
       snprintf(err, errlen, "pl_unet: workspace cudaMalloc(%zu) failed", bytes + fbytes);
@@ -575,6 +648,8 @@ struct UNetImpl {
     loss_part = (float*)p;
     p += size_t(nloss) * 4;
     loss = (float*)p;
+    p += 1024;
+    ad = (float*)p;
     return PL_OK;
   }
 
@@ -680,6 +755,12 @@ struct UNetImpl {
   }
 
   void loss_and_grad(const uint8_t* cell, const float* e, cudaStream_t st) {
+    if (loss_kind == PL_UNET_LOSS_ENERGY) {
+      k_energy_terms<<<b1.count, 256, 0, st>>>(b1, cell, o, e, scale, ad, energy, loss_part);
+      k_energy_grad<<<nb(b1.total(), 256), 256, 0, st>>>(b1, ad, scale, energy, d_o);
+      k_sum<<<1, 32, 0, st>>>(loss_part, b1.count, loss);
+      return;
+    }
     k_sample_stats<<<b1.count, 256, 0, st>>>(b1, cell, e, e, part, energy);  // energy of the targets
     k_loss<<<nb(b1.total(), 256), 256, 0, st>>>(b1, cell, o, e, scale, energy, d_o, loss_part);
     k_sum<<<1, 32, 0, st>>>(loss_part, nloss, loss);
@@ -711,6 +792,8 @@ UNetImpl* unet_create(uint32_t seed, char* err, size_t errlen, int* rc) {
 void unet_destroy(UNetImpl* u) { delete u; }
 
 int unet_nparams(const UNetImpl* u) { return u->nparam; }
+
+void unet_set_loss(UNetImpl* u, int kind) { u->loss_kind = kind; }
 
 int unet_get_params(UNetImpl* u, float* host) {
   return cudaMemcpy(host, u->param, size_t(u->nparam) * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? PL_OK

@@ -30,7 +30,8 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_destroy",
+    "pl_unet_set_loss",
+    "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
 
@@ -104,6 +105,7 @@ def lib() -> C.CDLL:
     L.pl_unet_gradient.argtypes = [P, P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, fp, P]
     L.pl_unet_destroy.argtypes = [P]
     L.pl_unet_destroy.restype = None
+    L.pl_unet_set_loss.argtypes = [P, C.c_int32]
     L.pl_get_affine.argtypes = [P, fp]
     L.pl_set_affine.argtypes = [P, fp]
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
@@ -116,6 +118,7 @@ def lib() -> C.CDLL:
     L.pl_poisson_set_unet.argtypes = [P, P]
     L.pl_poisson_device_bytes.argtypes = [P]
     L.pl_poisson_device_bytes.restype = C.c_size_t
+    L.pl_poisson_history.argtypes = [P, C.c_int32, dp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.pl_poisson_destroy.argtypes = [P]
     L.pl_poisson_destroy.restype = None
     _lib = L
@@ -425,6 +428,13 @@ class PoissonBatch:
                                       _ptr(conv, C.c_int32)))
         return it, res, conv.astype(bool)
 
+    def history(self, snapshot: int):
+        """(max|r| after each of the first 64 iterations of the last solve, iterations with the network)."""
+        out = np.zeros(64)
+        n, li = C.c_int32(), C.c_int32()
+        _check(lib().pl_poisson_history(self._h, snapshot, _ptr(out, C.c_double), 64, C.byref(n), C.byref(li)))
+        return out[:n.value].copy(), int(li.value)
+
     def destroy(self):
         if self._h:
             lib().pl_poisson_destroy(self._h)
@@ -441,6 +451,7 @@ class PoissonBatch:
 
 UNET_LAYERS = [(16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32), (32, 32), (48, 16), (16, 16),
                (16, 16)]  # (input, output) channels of the 11 convolutions, padded to multiples of 16
+UNET_LOSS_L2, UNET_LOSS_ENERGY = 0, 1
 
 
 class UNet:
@@ -451,6 +462,10 @@ class UNet:
         _check(lib().pl_unet_create(seed, C.byref(h)))
         self._h = h
         self.nparams = int(lib().pl_unet_num_params(h))
+
+    def set_loss(self, kind: int):
+        """UNET_LOSS_L2 (relative squared error) or UNET_LOSS_ENERGY (relative error in the energy norm)."""
+        _check(lib().pl_unet_set_loss(self._h, kind))
 
     def params(self) -> np.ndarray:
         out = np.zeros(self.nparams, np.float32)

@@ -23,12 +23,13 @@ def box_for(nx: int, ny: int, nz: int) -> tuple[int, int, int]:
 
 def apply_a(cell: np.ndarray, x: np.ndarray) -> np.ndarray:
     """A x of the Pcg3D operator on a (nz, ny, nx) box (FP64): non-SOLID neighbours count on the
-    diagonal, FLUID neighbours couple with -1; non-liquid and border cells are not unknowns."""
+    diagonal (+1 on a pinned cell), FLUID neighbours couple with -1; non-liquid and border cells are
+    not unknowns."""
     typ = cell & 3
     u = typ == FLUID
     u[0, :, :] = u[-1, :, :] = u[:, 0, :] = u[:, -1, :] = u[:, :, 0] = u[:, :, -1] = False
     xu = np.where(u, x, 0.0)
-    diag = np.zeros(cell.shape)
+    diag = ((cell & 4) != 0).astype(np.float64)  # the gauge pin (pl_poisson_gauge_fix)
     nsum = np.zeros(cell.shape)
     for axis in range(3):
         for sh in (1, -1):
@@ -69,6 +70,26 @@ def harvest_pour_systems(cell_mm: float = 5.0, count: int = 32, every: int = 12,
     return box, np.stack(cells), np.stack(rs), np.stack(es)
 
 
+def residual_pairs(box, cells: np.ndarray, r: np.ndarray, e: np.ndarray, iters=(1, 2, 3)):
+    """Residual/correction pairs of the plain multigrid PCG: for each system and each k in `iters`,
+    x_k after k iterations from zero, r_k = r - A x_k and e_k = e - x_k (so A e_k = r_k exactly, up to
+    FP32 rounding of the stored vectors). Together with the systems' own (r, e) they cover the
+    residuals the flexible CG hands the network in its later iterations. Returns (cells, r, e) with
+    the systems' pairs first, then those of each k."""
+    X, Y, Z = box
+    cs, rs, es = [cells], [r], [e]
+    for k in iters:
+        x, _, _, _ = solve(box, cells, r, E.POISSON_MG, tol=1e-30, max_iter=int(k))
+        rk = np.empty_like(r)
+        for i in range(cells.shape[0]):
+            ax = apply_a(cells[i].reshape(Z, Y, X), x[i].reshape(Z, Y, X)).reshape(-1)
+            rk[i] = (r[i].astype(np.float64) - ax).astype(np.float32)
+        cs.append(cells)
+        rs.append(rk)
+        es.append((e.astype(np.float64) - x).astype(np.float32))
+    return np.concatenate(cs), np.concatenate(rs), np.concatenate(es)
+
+
 def train(net: E.UNet, box, cells: np.ndarray, r: np.ndarray, e: np.ndarray, steps: int, batch: int = 4,
           lr: float = 1e-3, seed: int = 0, time_limit: float | None = None):
     """Adam steps on random batches of the pairs (device copies made once). Returns the loss history."""
@@ -95,9 +116,10 @@ def train(net: E.UNet, box, cells: np.ndarray, r: np.ndarray, e: np.ndarray, ste
 
 
 def solve(box, cells: np.ndarray, r: np.ndarray, method: int, tol: float = 1e-6, max_iter: int = 1000,
-          net: E.UNet | None = None, reps: int = 1):
+          net: E.UNet | None = None, reps: int = 1, history: list | None = None):
     """pl_poisson_solve of the systems (FP32 vectors, FP64 refinement); returns (x, iterations,
-    converged, ms of the fastest repetition)."""
+    converged, ms of the fastest repetition). A list passed as `history` receives, per system, the
+    max-norm residual after each iteration and the iterations taken with the network."""
     import torch
 
     count = cells.shape[0]
@@ -117,5 +139,7 @@ def solve(box, cells: np.ndarray, r: np.ndarray, method: int, tol: float = 1e-6,
         torch.cuda.synchronize()
         ms = a.elapsed_time(b)
         best = ms if best is None else min(best, ms)
+    if history is not None:
+        history.extend(pb.history(s) for s in range(count))
     pb.destroy()
     return dx.cpu().numpy(), it, conv, best

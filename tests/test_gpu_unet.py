@@ -22,6 +22,25 @@ def case(seed=3):
     return cell, r, e
 
 
+def exact_corrections(cell, r):
+    """e = A^-1 r on each box's unknowns (liquid cells off the border; dense FP64 solve), 0 elsewhere."""
+    from teapotfluidsimulation_b200 import learned as Lr
+
+    e = np.zeros(r.shape, np.float32)
+    for s in range(cell.shape[0]):
+        c = cell[s]
+        u = (c & 3) == 1
+        u[0] = u[-1] = u[:, 0] = u[:, -1] = u[:, :, 0] = u[:, :, -1] = False
+        unk = np.flatnonzero(u)
+        A = np.empty((unk.size, unk.size))
+        for n, i in enumerate(unk):
+            A[:, n] = Lr.apply_a(c, np.eye(1, c.size, i).reshape(c.shape)).reshape(-1)[unk]
+        es = np.zeros(c.size)
+        es[unk] = np.linalg.solve(A, r[s].reshape(-1)[unk].astype(np.float64))
+        e[s] = es.reshape(c.shape)
+    return e
+
+
 def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
@@ -42,13 +61,18 @@ def test_forward_matches_fp64_restatement(engine):
     assert rel < 3e-2, rel  # BF16 weights and activations through 11 layers
 
 
-def test_gradient_matches_fp64_restatement(engine):
+@pytest.mark.parametrize("energy", [False, True])
+def test_gradient_matches_fp64_restatement(engine, energy):
     cell, r, e = case()
+    if energy:  # the pairs the energy loss is meant for: e solves A e = r
+        e = exact_corrections(cell, r)
     net = engine.engine.UNet(seed=5)
+    if energy:
+        net.set_loss(engine.engine.UNET_LOSS_ENERGY)
     p = net.params()
     dc, dr, de = dev(cell), dev(r), dev(e)
     loss, g = net.gradient(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), NX, NY, NZ, N)
-    loss_ref, g_ref, _ = unet_ref.loss_and_grad(p.astype(np.float64), cell, r, e)
+    loss_ref, g_ref, _ = unet_ref.loss_and_grad(p.astype(np.float64), cell, r, e, energy=energy)
     assert abs(loss - loss_ref) < 2e-2 * abs(loss_ref)
     cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
     assert cos > 0.995, cos
@@ -58,7 +82,10 @@ def test_gradient_matches_fp64_restatement(engine):
         a, b = g[o:o + n], g_ref[o:o + n]
         o += n
         if np.linalg.norm(b) > 0:
-            assert np.linalg.norm(a - b) <= 0.1 * np.linalg.norm(b), (li, np.linalg.norm(a - b) / np.linalg.norm(b))
+            # the energy loss's output gradient 2 s A d is rough (the stencil of a difference), so its BF16
+            # copy loses more through the 11 layers to the first one
+            tol = 0.25 if energy else 0.1
+            assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b), (li, np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
 def test_training_lowers_the_loss(engine):

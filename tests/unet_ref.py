@@ -56,15 +56,44 @@ def forward(layers, cell, r):
     return z, s
 
 
-def loss_and_grad(params, cell, r, e):
+def apply_a(cell, x):
+    """The 7-point pressure operator on (N, Z, Y, X) boxes: unknowns are liquid cells off the border;
+    diagonal = non-SOLID neighbours (+1 on pinned cells), -1 between neighbouring unknowns."""
+    typ = cell & 3
+    u = typ == FLUID
+    u[:, 0] = u[:, -1] = u[:, :, 0] = u[:, :, -1] = u[:, :, :, 0] = u[:, :, :, -1] = False
+    ut = torch.tensor(u, dtype=torch.float64)
+    diag = torch.tensor((cell & 4) != 0, dtype=torch.float64)
+    ns = torch.tensor(typ != 2, dtype=torch.float64)
+    xu = x * ut
+    nsum = torch.zeros_like(x)
+    for axis in (1, 2, 3):
+        for sh in (1, -1):
+            diag = diag + torch.roll(ns, sh, axis)
+            nsum = nsum + torch.roll(xu, sh, axis)
+    return (diag * xu - nsum) * ut, ut
+
+
+def loss_and_grad(params, cell, r, e, energy=False):
+    """Loss of the network on (r, e) pairs and its gradient: the relative squared error over the liquid
+    cells, or (energy=True) the relative error in the operator's energy norm over the unknowns."""
     layers = unpack(params)
     z, _ = forward(layers, cell, r)
     liq = torch.tensor(cell == FLUID, dtype=torch.float64)
-    et = torch.tensor(e, dtype=torch.float64) * liq
     n = r.shape[0]
-    en = (et ** 2).sum(dim=(1, 2, 3))
-    en = torch.where(en > 0, en, torch.ones_like(en))
-    loss = (((z - et) ** 2).sum(dim=(1, 2, 3)) / en).sum() / n
+    if energy:
+        e64 = torch.tensor(e, dtype=torch.float64)
+        ae, ut = apply_a(cell, e64)
+        d = (z - e64) * ut
+        ad, _ = apply_a(cell, d)
+        en = (e64 * ut * ae).sum(dim=(1, 2, 3))
+        en = torch.where(en > 0, en, torch.ones_like(en))
+        loss = ((d * ad).sum(dim=(1, 2, 3)) / en).sum() / n
+    else:
+        et = torch.tensor(e, dtype=torch.float64) * liq
+        en = (et ** 2).sum(dim=(1, 2, 3))
+        en = torch.where(en > 0, en, torch.ones_like(en))
+        loss = (((z - et) ** 2).sum(dim=(1, 2, 3)) / en).sum() / n
     loss.backward()
     g = np.concatenate([np.concatenate([w.grad.numpy().reshape(-1), b.grad.numpy()]) for w, b in layers])
     return float(loss.detach()), g, z.detach().numpy()
