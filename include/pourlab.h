@@ -59,8 +59,19 @@ enum pl_phase {
  * applied in wavefront order on the device; MG is a 3D geometric multigrid V-cycle (the 3D form
  * of src/sim/multigrid.ts with a red-black Gauss-Seidel smoother); CHEB is the Chebyshev
  * polynomial of the WebGPU port (src/gpu3d/shaders.ts:588-622). MG and CHEB run on one
- * 16-CTA thread-block cluster with the vectors in distributed shared memory. */
-enum pl_preconditioner { PL_PRECOND_MIC0 = 0, PL_PRECOND_MG = 1, PL_PRECOND_CHEB = 2 };
+ * 16-CTA thread-block cluster with the vectors in distributed shared memory, for systems up to
+ * about 65k liquid cells (larger ones fall back to the single-block MIC(0) solve).
+ * BOX_MG and LEARNED are the grid-scale solves, for any system size: the liquid system is embedded
+ * in a dense power-of-two box around the grid and solved there by multigrid PCG (the Poisson
+ * batch's Galerkin hierarchy) or by flexible CG with the network of pl_set_unet and that
+ * multigrid as the fall-back, the whole solve a while-loop node of the substep's CUDA graph. */
+enum pl_preconditioner {
+  PL_PRECOND_MIC0 = 0,
+  PL_PRECOND_MG = 1,
+  PL_PRECOND_CHEB = 2,
+  PL_PRECOND_BOX_MG = 3,
+  PL_PRECOND_LEARNED = 4
+};
 /* Arithmetic of the pressure solves: F64 keeps every solver vector in FP64; MIXED keeps the
  * Krylov and smoother vectors in FP32 with FP64 inner products, an FP64 solution and FP64
  * iterative refinement of the true residual. */
@@ -447,6 +458,9 @@ int pl_unet_train_step(pl_unet* u, const uint8_t* cell, const float* r, const fl
 int pl_unet_gradient(pl_unet* u, const uint8_t* cell, const float* r, const float* e, int32_t nx, int32_t ny,
                      int32_t nz, int32_t count, float* loss, float* grad, void* stream);
 void pl_unet_destroy(pl_unet* u);
+/* The network of a simulation created with PL_PRECOND_LEARNED (required before its first substep;
+ * the caller keeps it alive while the simulation uses it). Rebuilds the substep graph. */
+int pl_set_unet(pl_sim* sim, pl_unet* u);
 
 #ifdef __cplusplus
 }

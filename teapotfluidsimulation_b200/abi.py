@@ -22,7 +22,7 @@ MOTION_STILL, MOTION_POUR, MOTION_TILT, MOTION_MANUAL = 0, 1, 2, 3
 MOTION_KINDS = {"still": MOTION_STILL, "pour": MOTION_POUR, "tilt": MOTION_TILT, "manual": MOTION_MANUAL}
 PHASES = ["wait", "tilt-in", "hold", "return", "rest", "done", "manual"]
 
-PRECOND_MIC0, PRECOND_MG, PRECOND_CHEB = 0, 1, 2
+PRECOND_MIC0, PRECOND_MG, PRECOND_CHEB, PRECOND_BOX_MG, PRECOND_LEARNED = 0, 1, 2, 3, 4
 SOLVE_F64, SOLVE_MIXED = 0, 1
 TRANSFER_FLIP, TRANSFER_APIC = 0, 1
 DOMAIN_HALF, DOMAIN_FULL = 0, 1

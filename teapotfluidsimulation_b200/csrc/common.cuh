@@ -63,6 +63,8 @@ struct Geo {
   int tiled;     // the cluster solver orders its cells by column tile (ntx * nty * nz <= TILE_PLANES_MAX)
   int apic;      // affine particle-grid transfer (PL_TRANSFER_APIC)
   int full;      // both halves of the pot, no symmetry plane (PL_DOMAIN_FULL)
+  int box_solve;      // grid-scale pressure solves (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED)
+  int bx, by, bz;     // their power-of-two box (>= the grid, every side >= 8)
   double zoff;   // world z of the pot-local plane z = 0 (h for the half domain)
   double vol_factor;  // parcels' volume scale in the accounting: 2 (the half stands for the pot), 1 (full)
   double parcel_volume;
@@ -284,6 +286,12 @@ struct DevPtrs {
   uint8_t* occ;  // cell holds in-pot parcels
   float2* m_vel;
   float* m_den;
+  // grid-scale solves: the liquid system embedded in the box (cell types, rhs), the box solution and
+  // the solve's outcome (iterations, converged, max-norm residual)
+  uint8_t* box_cell;
+  float* box_b;
+  double* box_x;
+  double* box_out;
   // render
   float* render;
   SimScalars* sc;

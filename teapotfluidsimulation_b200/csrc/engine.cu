@@ -66,6 +66,8 @@ struct pl_sim {
   int timing = 0;
   int pending = 0;  // substeps queued by pl_enqueue_substeps since the last pull
   cudaEvent_t ev[PL_STAGES + 1] = {};
+  pl::PoissonImpl* box = nullptr;  // grid-scale solver (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED)
+  pl::UNetImpl* net = nullptr;     // its network (PL_PRECOND_LEARNED), owned by the caller
 };
 
 namespace {
@@ -98,7 +100,7 @@ int push_scalars(pl_sim* s) {
 
 // One substep, stage by stage; with timing on, an event is recorded at every stage boundary (event
 // record nodes inside the graph).
-void record_substep(pl_sim* s) {
+int record_substep(pl_sim* s) {
   const Geo& g = s->g;
   const DevPtrs& P = s->P;
   cudaStream_t st = s->st;
@@ -114,14 +116,24 @@ void record_substep(pl_sim* s) {
   mark(2);
   launch_stage_density(g, P, st);
   mark(3);
-  launch_pressure_solve(g, P, st);
+  char err[256] = "";
+  if (g.box_solve) {
+    if (launch_box_pressure(g, P, s->box, st, err, sizeof err)) return fail(PL_E_CUDA, "%s", err);
+  } else {
+    launch_pressure_solve(g, P, st);
+  }
   mark(4);
-  launch_correction_solve(g, P, st);
+  if (g.box_solve) {
+    if (launch_box_correction(g, P, s->box, st, err, sizeof err)) return fail(PL_E_CUDA, "%s", err);
+  } else {
+    launch_correction_solve(g, P, st);
+  }
   mark(5);
   launch_stage_extrap(g, P, st);
   mark(6);
   launch_stage_advect(g, P, st);
   mark(7);
+  return PL_OK;
 }
 
 // Event interval [first, second] of each stage (enum pl_stage order) in the execution order above.
@@ -132,10 +144,16 @@ int build_graph(pl_sim* s) {
     cudaGraphExecDestroy(s->exec);
     s->exec = nullptr;
   }
+  if (s->g.box_solve && s->cfg.preconditioner == PL_PRECOND_LEARNED && !s->net) return PL_OK;  // pl_set_unet
   cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-  record_substep(s);
-  CK(cudaStreamEndCapture(s->st, &graph));
+  const int rc = record_substep(s);
+  const cudaError_t ce = cudaStreamEndCapture(s->st, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (ce != cudaSuccess) return fail(PL_E_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ce));
   cudaError_t e = cudaGraphInstantiate(&s->exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return fail(PL_E_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
@@ -268,7 +286,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
     return fail(PL_E_CUDA, "pl_create: stream, events or pinned staging: %s", cudaGetErrorString(e));
   }
   // one allocation for everything
-  const size_t N = g.n, C = g.nc, F = g.nf, B = g.nbins + 1;
+  const size_t N = g.n, C = g.nc, F = g.nf, B = g.nbins + 1, NB = size_t(g.bx) * g.by * g.bz;
   size_t sizes[] = {
       N * 16, N * 16, N * 16, N * 16, N * 16, N * 16,  // pos/vel home, pos/vel sorted, frac sorted/tmp
       N * 4,  N * 4,  N * 8,                           // key, rank, placed
@@ -287,6 +305,8 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       C * 6 * 4, C * 4,                                // tile-order neighbours, permutation
       C, C * 3 * 27 * 8, C * 27 * 4,                   // occupancy, node partials (velocity, density)
       g.apic ? N * 48 : 16, g.apic ? N * 48 : 16,      // APIC affine vectors (home, sorted)
+      g.box_solve ? NB : 16, g.box_solve ? NB * 4 : 16,  // grid-scale solves: box cells, rhs
+      g.box_solve ? NB * 8 : 16, 32,                     // box solution, outcome
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -345,6 +365,21 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.m_den = (float*)take();
   P.aff_home = (float4*)take();
   P.aff_sorted = (float4*)take();
+  P.box_cell = (uint8_t*)take();
+  P.box_b = (float*)take();
+  P.box_x = (double*)take();
+  P.box_out = (double*)take();
+  if (g.box_solve) {
+    int brc = 0;
+    char berr[256] = "";
+    s->box = pl::poisson_create(g.bx, g.by, g.bz, 1,
+                                cfg->preconditioner == PL_PRECOND_LEARNED ? PL_POISSON_LEARNED : PL_POISSON_MG,
+                                g.precision, berr, sizeof berr, &brc);
+    if (!s->box) {
+      pl_destroy(s);
+      return fail(brc ? brc : PL_E_CUDA, "pl_create: grid-scale solver: %s", berr);
+    }
+  }
   mg_configure();
   cheb_configure();
   int nn = g.n;
@@ -406,6 +441,7 @@ void pl_destroy(pl_sim* s) {
   cudaSetDevice(s->device);
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
+  if (s->box) pl::poisson_destroy(s->box);
   if (s->mem) cudaFree(s->mem);
   for (int i = 0; i <= PL_STAGES; i++)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);
@@ -416,6 +452,7 @@ void pl_destroy(pl_sim* s) {
 
 int pl_enqueue_substeps(pl_sim* s, int32_t count) {
   if (!s || count < 0) return fail(PL_E_ARG, "pl_enqueue_substeps: bad argument");
+  if (!s->exec) return fail(PL_E_STATE, "pl_enqueue_substeps: the learned preconditioner needs a network (pl_set_unet)");
   cudaSetDevice(s->device);
   s->hs.end_time = INFINITY;  // run until finished
   s->hs.force_step = 0;
@@ -538,6 +575,7 @@ int pl_step(pl_sim* s, double dt) {
   if (rc) return rc;
   s->hs.force_step = 1;
   s->hs.forced_dt = dt > 0 ? dt : 0;
+  if (!s->exec) return fail(PL_E_STATE, "pl_step: the learned preconditioner needs a network (pl_set_unet)");
   rc = push_scalars(s);
   if (rc) return rc;
   CK(cudaGraphLaunch(s->exec, s->st));
@@ -549,6 +587,7 @@ int pl_advance(pl_sim* s, double duration, pl_diagnostics* out) {
   cudaSetDevice(s->device);
   int rc = settle(s);
   if (rc) return rc;
+  if (!s->exec) return fail(PL_E_STATE, "pl_advance: the learned preconditioner needs a network (pl_set_unet)");
   const double end = s->hs.time + duration;  // solver3d.ts:282
   s->hs.end_time = end;
   s->hs.force_step = 0;
@@ -974,6 +1013,21 @@ int pl_poisson_solve(pl_poisson* h, const uint8_t* cell, const float* b, double*
                              err, sizeof err);
   if (rc) return fail(rc, "%s", err);
   return PL_OK;
+}
+
+int pl_set_unet(pl_sim* s, pl_unet* u) {
+  if (!s || !u) return fail(PL_E_ARG, "pl_set_unet: null argument");
+  if (s->cfg.preconditioner != PL_PRECOND_LEARNED)
+    return fail(PL_E_STATE, "pl_set_unet: the simulation was not created with PL_PRECOND_LEARNED");
+  cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
+  char err[256] = "";
+  rc = pl::unet_prepare(u->impl, s->g.bx, s->g.by, s->g.bz, 1, err, sizeof err);  // workspace before the capture
+  if (rc) return fail(rc, "%s", err);
+  s->net = u->impl;
+  pl::poisson_set_unet(s->box, u->impl);
+  return build_graph(s);
 }
 
 int pl_poisson_set_unet(pl_poisson* h, pl_unet* u) {

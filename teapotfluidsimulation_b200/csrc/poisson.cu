@@ -347,9 +347,9 @@ __device__ __forceinline__ void row_sum(const T* x, const uint8_t* diag, const T
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                    const T* w, const T* dg, int cells, T* x, const T* b,
-                                                   int color, int first, const Snap* st, int nact) {
+                                                   int color, int first, const Snap* st, const int* nact) {
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
-  if (ti >= nact) return;
+  if (ti >= *nact) return;
   const int gt = list[ti];
   const int s = gt >> G.lnt;
   if (st[s].done) return;
@@ -378,9 +378,9 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* listc, const uint8_t* codef,
                                                      const uint8_t* diagf, const T* wf, const T* dgf, int cellsf,
                                                      const T* xf, const T* bf, const uint8_t* codec, T* bc,
-                                                     const Snap* st, int nact) {
+                                                     const Snap* st, const int* nact) {
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
-  if (ti >= nact) return;
+  if (ti >= *nact) return;
   const int gt = listc[ti];
   if (st[gt >> Gc.lnt].done) return;
   const int rx = Gc.rx, ry = Gc.ry, rz = Gc.rz, nxf = Gf.nx, nxyf = Gf.nx * Gf.ny;
@@ -411,9 +411,9 @@ __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* lis
 // Two tiles per CTA, two cells per thread.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* listf, const uint8_t* codef, T* xf,
-                                                    const uint8_t* codec, const T* xc, const Snap* st, int nact) {
+                                                    const uint8_t* codec, const T* xc, const Snap* st, const int* nact) {
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
-  if (ti >= nact) return;
+  if (ti >= *nact) return;
   const int gt = listf[ti];
   if (st[gt >> Gf.lnt].done) return;
 #pragma unroll
@@ -581,7 +581,7 @@ __device__ __forceinline__ void half_store(double v, double* out, bool is_max) {
 // partial per tile.
 #define PCG_TILE_PROLOGUE                                   \
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);       \
-  const bool has = ti < nact;                               \
+  const bool has = ti < *nact;                              \
   const int gt = has ? list[ti] : 0;                        \
   const int snap = gt >> G.lnt;                             \
   const bool live = has && !st[snap].done;
@@ -589,7 +589,7 @@ __device__ __forceinline__ void half_store(double v, double* out, bool is_max) {
 // r = b, x = 0, p = 0, |b| max per snapshot.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_init(TG G, const int* list, const uint8_t* code, const float* b, T* r,
-                                                 double* x, T* p, double* part, const Snap* st, int nact) {
+                                                 double* x, T* p, double* part, const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   double v = 0;
   if (has) {
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(PT) k_pcg_init(TG G, const int* list, const ui
 // Partial z.r per tile; with r_old (flexible CG) also z.r_old into part2.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint8_t* code, const T* r, const T* z,
-                                               const T* rold, double* part, double* part2, const Snap* st, int nact) {
+                                               const T* rold, double* part, double* part2, const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   double v = 0, v2 = 0;
   if (live) {
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint
 // Learned preconditioning: z = the network's output zn on the snapshots that still use it.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_select_pre(TG G, const int* list, const uint8_t* code, const float* zn, T* z,
-                                                   const Snap* st, int nact) {
+                                                   const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   if (!live || st[snap].pre) return;
 #pragma unroll
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(PT) k_select_pre(TG G, const int* list, const 
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                 const T* z, const T* pold, T* pnew, T* ap, double* part,
-                                                const Snap* st, int nact) {
+                                                const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   double v = 0;
   if (live) {
@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uin
 // x += alpha p, r -= alpha Ap; max |r| per tile.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const uint8_t* code, double* x, const T* p,
-                                                   T* r, const T* ap, T* rold, double* part, const Snap* st, int nact) {
+                                                   T* r, const T* ap, T* rold, double* part, const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   double v = 0;
   if (live) {
@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const 
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                  const float* b, const double* x, T* r, double* part,
-                                                 const Snap* st, int nact) {
+                                                 const Snap* st, const int* nact) {
   PCG_TILE_PROLOGUE
   const bool chk = live && st[snap].check;
   double v = 0;
@@ -822,12 +822,24 @@ __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* p
   }
 }
 
-__global__ void k_pcg_alldone(const Snap* st, int count, int* out) {
-  int all = 1;
+__global__ void k_snap_result(const Snap* st, double* out) {
+  out[0] = st[0].it;
+  out[1] = st[0].converged;
+  out[2] = st[0].res;
+}
+
+// Control of the iteration loop (a graph while-node): another pass while a snapshot is live, and never
+// more than `cap` passes (every snapshot stops at its iteration cap well before; the count is a hard
+// bound on the loop whatever the state holds).
+__global__ void k_loop_next(const Snap* st, int count, int* passes, int cap, cudaGraphConditionalHandle h) {
+  int live = 0;
   for (int s = threadIdx.x; s < count; s += blockDim.x)
-    if (!st[s].done) all = 0;
-  all = __syncthreads_and(all);
-  if (threadIdx.x == 0) *out = all;
+    if (!st[s].done) live = 1;
+  live = __syncthreads_or(live);
+  if (threadIdx.x == 0) {
+    const int q = ++*passes;
+    cudaGraphSetConditional(h, (live && q < cap) ? 1u : 0u);
+  }
 }
 
 }  // namespace
@@ -839,6 +851,10 @@ struct PoissonImpl {
   UNetImpl* net = nullptr;  // learned preconditioning (PL_POISSON_LEARNED), owned by the caller
   virtual int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t st,
                     int* iters, double* res, int* conv, char* err, size_t errlen) = 0;
+  virtual int capture_setup(const uint8_t* cell, cudaStream_t st, char* err, size_t errlen) = 0;
+  virtual int capture_solve(const float* b, double* x, double tol, int max_iter, cudaStream_t st, char* err,
+                            size_t errlen) = 0;
+  virtual void capture_result(double* out3, cudaStream_t st) = 0;
   size_t bytes = 0;
   std::vector<Snap> last;  // per-snapshot state at the end of the last solve
 };
@@ -857,14 +873,24 @@ struct PoissonT : PoissonImpl {
   const uint8_t* cell_in = nullptr;
   double *part = nullptr, *part2 = nullptr;
   Snap* st = nullptr;
-  int* dcnt = nullptr;  // [PMAXLEV] active tile counters, [PMAXLEV] all-done flag
+  int* dcnt = nullptr;  // [PMAXLEV] active tile counters, then the loop's pass counter
+  int* passes = nullptr;
+  cudaStream_t side = nullptr;  // captures the loop body
   int* chunk = nullptr;  // per-chunk counts / offsets of the list compaction
   int* pinned = nullptr;
   cudaGraphExec_t iter_graph = nullptr;
   static unsigned grid2(int nact) { return unsigned(std::max(1, (nact + 1) / 2)); }  // two tiles per CTA
+  // Device-driven mode: the active tile counts stay on the device (every launch is sized for all
+  // tiles and its CTAs past the count return at once) and the iterations run as a graph while-loop,
+  // so a whole solve can be captured into a caller's graph.
+  bool devmode = false;
+  int lim(int l) const { return devmode ? int(count * L[l].G.ntile) : L[l].nact; }
+  bool any(int l) const { return devmode || L[l].nact > 0; }
+  const int* nact_d(int l) const { return dcnt + l; }
 
   ~PoissonT() override {
     if (iter_graph) cudaGraphExecDestroy(iter_graph);
+    if (side) cudaStreamDestroy(side);
     if (mem) cudaFree(mem);
     if (pinned) cudaFreeHost(pinned);
   }
@@ -951,6 +977,7 @@ struct PoissonT : PoissonImpl {
     zn = learned() ? (float*)at[i_zn] : nullptr;
     st = (Snap*)at[i_st];
     dcnt = (int*)at[i_cnt];
+    passes = dcnt + PMAXLEV;
     chunk = (int*)at[i_chunk];
     e = cudaMemset(mem, 0, total);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&pinned, 4 * (PMAXLEV + 1), cudaHostAllocDefault);
@@ -961,8 +988,8 @@ struct PoissonT : PoissonImpl {
     return PL_OK;
   }
 
-  // Level types, codes, tile lists; the MIC(0) factor.
-  int setup(const uint8_t* cell, cudaStream_t s0) {
+  // Level types, codes, Galerkin operators and active tile lists (counts left on the device).
+  void build_levels(const uint8_t* cell, cudaStream_t s0) {
     for (int l = 0; l < nlev; l++) {
       const TG& G = L[l].G;
       const long long nt = (long long)count * G.ntile;
@@ -980,6 +1007,11 @@ struct PoissonT : PoissonImpl {
       k_compact_scan<<<1, CHUNK, 0, s0>>>(chunk, nchunk, dcnt + l);
       k_compact_write<<<nchunk, CHUNK, 0, s0>>>(L[l].flag, nt, chunk, L[l].list);
     }
+  }
+
+  // Host-driven set-up: the levels, their active tile counts read back, the MIC(0) factor.
+  int setup(const uint8_t* cell, cudaStream_t s0) {
+    build_levels(cell, s0);
     cudaMemcpyAsync(pinned, dcnt, 4 * PMAXLEV, cudaMemcpyDeviceToHost, s0);
     cudaError_t e = cudaStreamSynchronize(s0);
     if (e != cudaSuccess) return PL_E_CUDA;
@@ -1001,15 +1033,14 @@ struct PoissonT : PoissonImpl {
     char err[128];
     const TG& G = L[0].G;
     unet_apply(net, cell_in, reinterpret_cast<const float*>(r), zn, G.nx, G.ny, G.nz, count, s0, err, sizeof err);
-    k_select_pre<T><<<grid2(L[0].nact), PT, 0, s0>>>(G, L[0].list, L[0].code, zn, z, st, L[0].nact);
+    k_select_pre<T><<<grid2(lim(0)), PT, 0, s0>>>(G, L[0].list, L[0].code, zn, z, st, nact_d(0));
     // the network's correction, then red-black Gauss-Seidel sweeps from it: the network carries the
     // smooth part of the error, the sweeps the rough part (on a fallen-back snapshot they follow the
     // V-cycle's own post-smoothing)
     for (int q = 0; q < MG_NU; q++)
       for (int color = 0; color < 2; color++)
-        k_mg_smooth<T><<<unsigned((L[0].nact + 1) / 2), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, L[0].w,
-                                                                     L[0].dg, int(count * G.nc), z, r, color, 0, st,
-                                                                     L[0].nact);
+        k_mg_smooth<T><<<grid2(lim(0)), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
+                                                     int(count * G.nc), z, r, color, 0, st, nact_d(0));
   }
 
   void mg_or_mic0(cudaStream_t s0) {
@@ -1025,23 +1056,22 @@ struct PoissonT : PoissonImpl {
     auto B = [&](int l) -> const T* { return l == 0 ? r : L[l].b; };
     auto cells = [&](int l) { return (long long)count * L[l].G.nc; };
     auto smooth = [&](int l, int color, int first) {
-      k_mg_smooth<T><<<unsigned((L[l].nact + 1) / 2), PT, 0, s0>>>(L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w,
-                                                                   L[l].dg, cells(l), X(l), B(l), color, first, st,
-                                                                   L[l].nact);
+      k_mg_smooth<T><<<grid2(lim(l)), PT, 0, s0>>>(L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
+                                                   cells(l), X(l), B(l), color, first, st, nact_d(l));
     };
     const int top = nlev - 1;
     for (int l = 0; l < top; l++) {
-      if (L[l].nact == 0) continue;
+      if (!any(l)) continue;
       for (int q = 0; q < MG_NU; q++) {
         smooth(l, 0, q == 0);
         smooth(l, 1, 0);
       }
-      if (L[l + 1].nact)
-        k_mg_restrict<T><<<grid2(L[l + 1].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
-                                                             L[l].w, L[l].dg, cells(l), X(l), B(l), L[l + 1].code,
-                                                             L[l + 1].b, st, L[l + 1].nact);
+      if (any(l + 1))
+        k_mg_restrict<T><<<grid2(lim(l + 1)), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
+                                                          L[l].w, L[l].dg, cells(l), X(l), B(l), L[l + 1].code,
+                                                          L[l + 1].b, st, nact_d(l + 1));
     }
-    if (L[top].nact) {
+    if (any(top)) {
       if (top == 0 || L[top].G.nc > 512) {  // no level small enough for one CTA: plain red-black sweeps
         for (int q = 0; q < COARSE_SWEEPS; q++) {
           smooth(top, 0, q == 0);
@@ -1057,10 +1087,10 @@ struct PoissonT : PoissonImpl {
       }
     }
     for (int l = top - 1; l >= 0; l--) {
-      if (L[l].nact == 0) continue;
-      if (L[l + 1].nact)
-        k_mg_prolong<T><<<grid2(L[l].nact), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
-                                                        L[l + 1].code, L[l + 1].x, st, L[l].nact);
+      if (!any(l)) continue;
+      if (any(l + 1))
+        k_mg_prolong<T><<<grid2(lim(l)), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
+                                                     L[l + 1].code, L[l + 1].x, st, nact_d(l));
       for (int q = 0; q < MG_NU; q++) {
         smooth(l, 1, 0);
         smooth(l, 0, 0);
@@ -1072,20 +1102,96 @@ struct PoissonT : PoissonImpl {
   // preconditioner first: z = M r, beta, p and Ap, alpha, update, convergence / true residual).
   void iteration(const float* b, double* x, double tol, int max_iter, T* pold, T* pnew, cudaStream_t s0) {
     const TG& G = L[0].G;
-    const int na = L[0].nact;
+    const unsigned g0 = grid2(lim(0));
+    const int* na = nact_d(0);
     precondition(s0);
-    k_pcg_rz<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, rold, part, part2, st, na);
+    k_pcg_rz<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, rold, part, part2, st, na);
     k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_pap<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
+    k_pcg_pap<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
     k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_update<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, rold, part, st, na);
+    k_pcg_update<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, rold, part, st, na);
     k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_true<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
+    k_pcg_true<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
     k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, part2, G.ntile, st, tol, max_iter, learned());
   }
 
+  // r = b, x = 0, p = p1 = 0 and the per-snapshot state (enqueued on s0, capturable).
+  void start(const float* b, double* x, double tol, int max_iter, cudaStream_t s0) {
+    const TG& G = L[0].G;
+    cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);  // inactive tiles' partials stay 0
+    cudaMemsetAsync(x, 0, size_t(count) * G.nc * 8, s0);
+    cudaMemsetAsync(p1, 0, size_t(count) * G.nc * sizeof(T), s0);
+    if (learned()) cudaMemsetAsync(rold, 0, size_t(count) * G.nc * sizeof(T), s0);
+    cudaMemsetAsync(passes, 0, 4, s0);
+    if (any(0)) k_pcg_init<T><<<grid2(lim(0)), PT, 0, s0>>>(G, L[0].list, L[0].code, b, r, x, p, part, st, nact_d(0));
+    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, part2, G.ntile, st, tol, max_iter, learned());
+  }
+
+  // The iterations as a while-node of the graph being captured on s0: its body (two iterations, the
+  // search direction alternating between p and p1, then the loop control) is captured on a private
+  // stream into the node's body graph.
+  int record_loop(const float* b, double* x, double tol, int max_iter, cudaStream_t s0, char* err, size_t errlen) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s0, &cs, nullptr, &cg, &deps, &nd);
+    if (e == cudaSuccess && cs != cudaStreamCaptureStatusActive) e = cudaErrorStreamCaptureUnmatched;
+    cudaGraphConditionalHandle h{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, cg, deps, nd, &np);
+    if (e == cudaSuccess && !side) e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = np.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+      if (e == cudaSuccess) {
+        iteration(b, x, tol, max_iter, p, p1, side);
+        iteration(b, x, tol, max_iter, p1, p, side);
+        k_loop_next<<<1, 256, 0, side>>>(st, count, passes, max_iter / 2 + 8, h);
+        e = cudaStreamEndCapture(side, &body);
+      }
+    }
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s0, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "pl_poisson: iteration loop: %s", cudaGetErrorString(e));
+      return PL_E_CUDA;
+    }
+    return PL_OK;
+  }
+
+  // Device-driven use inside a caller's capture on s0: the levels of `cell` (once per cell layout),
+  // then any number of solves on it. No host synchronisation; results stay in the snapshot state.
+  int capture_setup(const uint8_t* cell, cudaStream_t s0, char* err, size_t errlen) override {
+    if (method == PL_POISSON_MIC0) {
+      snprintf(err, errlen, "pl_poisson: the device-driven solve is multigrid or learned");
+      return PL_E_ARG;
+    }
+    devmode = true;
+    cell_in = cell;
+    build_levels(cell, s0);
+    return PL_OK;
+  }
+  int capture_solve(const float* b, double* x, double tol, int max_iter, cudaStream_t s0, char* err,
+                    size_t errlen) override {
+    if (learned() && !net) {
+      snprintf(err, errlen, "pl_poisson: the learned method needs a network");
+      return PL_E_STATE;
+    }
+    start(b, x, tol, max_iter, s0);
+    return record_loop(b, x, tol, max_iter, s0, err, errlen);
+  }
+  // The first snapshot's outcome (iterations, converged, max-norm residual) to device memory.
+  void capture_result(double* out3, cudaStream_t s0) override { k_snap_result<<<1, 1, 0, s0>>>(st, out3); }
+
   int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t s0, int* iters,
             double* res, int* conv, char* err, size_t errlen) override {
+    devmode = false;
     int rc = setup(cell, s0);
     if (rc) {
       snprintf(err, errlen, "pl_poisson_solve: set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1099,53 +1205,36 @@ struct PoissonT : PoissonImpl {
       }
       rc = unet_prepare(net, L[0].G.nx, L[0].G.ny, L[0].G.nz, count, err, errlen);  // before the capture
       if (rc) return rc;
-      cudaMemsetAsync(rold, 0, size_t(count) * L[0].G.nc * sizeof(T), s0);
     }
-    const TG& G = L[0].G;
-    const int na = L[0].nact;
-    cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);  // inactive tiles' partials stay 0
-    cudaMemsetAsync(x, 0, size_t(count) * G.nc * 8, s0);
-    if (na > 0) k_pcg_init<T><<<grid2(na), PT, 0, s0>>>(G, L[0].list, L[0].code, b, r, x, p, part, st, na);
-    cudaMemsetAsync(p1, 0, size_t(count) * G.nc * sizeof(T), s0);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(0, part, part2, G.ntile, st, tol, max_iter, learned());
-    if (na > 0) {
-      // the iteration as a CUDA graph (one launch per iteration), checked for completion in batches
-      if (iter_graph) {
-        cudaGraphExecDestroy(iter_graph);
-        iter_graph = nullptr;
-      }
-      cudaGraph_t gph = nullptr;
-      cudaStream_t cap = nullptr;
-      cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-      if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-      if (e == cudaSuccess) {  // two iterations, the search direction alternating between p and p1
-        iteration(b, x, tol, max_iter, p, p1, cap);
-        iteration(b, x, tol, max_iter, p1, p, cap);
-        e = cudaStreamEndCapture(cap, &gph);
-      }
-      if (e == cudaSuccess) e = cudaGraphInstantiate(&iter_graph, gph, 0);
-      if (gph) cudaGraphDestroy(gph);
-      if (cap) cudaStreamDestroy(cap);
-      if (e != cudaSuccess) {
-        snprintf(err, errlen, "pl_poisson_solve: iteration graph: %s", cudaGetErrorString(e));
-        return PL_E_CUDA;
-      }
-      const int batch = 4;  // graph launches (8 iterations) between completion checks
-      for (int done_it = 0; done_it < max_iter + 8;) {
-        for (int q = 0; q < batch; q++) cudaGraphLaunch(iter_graph, s0);
-        done_it += 2 * batch;
-        k_pcg_alldone<<<1, 256, 0, s0>>>(st, count, dcnt + PMAXLEV);
-        cudaMemcpyAsync(pinned + PMAXLEV, dcnt + PMAXLEV, 4, cudaMemcpyDeviceToHost, s0);
-        e = cudaStreamSynchronize(s0);
-        if (e != cudaSuccess) {
-          snprintf(err, errlen, "pl_poisson_solve: %s", cudaGetErrorString(e));
-          return PL_E_CUDA;
-        }
-        if (pinned[PMAXLEV]) break;
-      }
+    // the whole solve as one graph (start, then the iteration loop), launched once
+    if (iter_graph) {
+      cudaGraphExecDestroy(iter_graph);
+      iter_graph = nullptr;
+    }
+    cudaGraph_t gph = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      start(b, x, tol, max_iter, cap);
+      rc = any(0) ? record_loop(b, x, tol, max_iter, cap, err, errlen) : PL_OK;
+      e = cudaStreamEndCapture(cap, &gph);
+      if (rc) e = cudaErrorUnknown;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&iter_graph, gph, 0);
+    if (gph) cudaGraphDestroy(gph);
+    if (cap) cudaStreamDestroy(cap);
+    if (e != cudaSuccess) {
+      if (!rc) snprintf(err, errlen, "pl_poisson_solve: solve graph: %s", cudaGetErrorString(e));
+      return rc ? rc : PL_E_CUDA;
+    }
+    e = cudaGraphLaunch(iter_graph, s0);
+    if (e != cudaSuccess) {
+      snprintf(err, errlen, "pl_poisson_solve: %s", cudaGetErrorString(e));
+      return PL_E_CUDA;
     }
     std::vector<Snap> hs(count);
-    cudaError_t e = cudaMemcpyAsync(hs.data(), st, sizeof(Snap) * count, cudaMemcpyDeviceToHost, s0);
+    e = cudaMemcpyAsync(hs.data(), st, sizeof(Snap) * count, cudaMemcpyDeviceToHost, s0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s0);
     if (e != cudaSuccess) {
       snprintf(err, errlen, "pl_poisson_solve: %s", cudaGetErrorString(e));
@@ -1394,6 +1483,17 @@ void poisson_destroy(PoissonImpl* h) { delete h; }
 void poisson_set_unet(PoissonImpl* h, UNetImpl* u) { h->net = u; }
 
 size_t poisson_bytes(const PoissonImpl* h) { return h ? h->bytes : 0; }
+
+int poisson_capture_setup(PoissonImpl* h, const uint8_t* cell, cudaStream_t st, char* err, size_t errlen) {
+  return h->capture_setup(cell, st, err, errlen);
+}
+
+int poisson_capture_solve(PoissonImpl* h, const float* b, double* x, double tol, int max_iter, cudaStream_t st,
+                          char* err, size_t errlen) {
+  return h->capture_solve(b, x, tol, max_iter, st, err, errlen);
+}
+
+void poisson_capture_result(PoissonImpl* h, double* out3, cudaStream_t st) { h->capture_result(out3, st); }
 
 int poisson_history(const PoissonImpl* h, int snapshot, double* out, int capacity, int* recorded, int* learned_it) {
   if (snapshot < 0 || snapshot >= (int)h->last.size()) return PL_E_ARG;

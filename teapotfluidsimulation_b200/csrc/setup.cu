@@ -222,6 +222,27 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
     return PL_E_ARG;
   }
   g.apic = cfg.transfer == PL_TRANSFER_APIC ? 1 : 0;
+  if (cfg.preconditioner < PL_PRECOND_MIC0 || cfg.preconditioner > PL_PRECOND_LEARNED) {
+    snprintf(err, errlen, "pl_create: unknown preconditioner %d", cfg.preconditioner);
+    return PL_E_ARG;
+  }
+  if (cfg.solve_precision != PL_SOLVE_F64 && cfg.solve_precision != PL_SOLVE_MIXED) {
+    snprintf(err, errlen, "pl_create: unknown solve precision %d", cfg.solve_precision);
+    return PL_E_ARG;
+  }
+  if (cfg.preconditioner == PL_PRECOND_LEARNED && cfg.solve_precision != PL_SOLVE_MIXED) {
+    snprintf(err, errlen, "pl_create: the learned preconditioner runs with FP32 vectors (PL_SOLVE_MIXED)");
+    return PL_E_ARG;
+  }
+  g.box_solve = (cfg.preconditioner == PL_PRECOND_BOX_MG || cfg.preconditioner == PL_PRECOND_LEARNED) ? 1 : 0;
+  {
+    auto p2 = [](int v) {
+      int b = 8;
+      while (b < v) b *= 2;
+      return b;
+    };
+    g.bx = p2(g.nx), g.by = p2(g.ny), g.bz = p2(g.nz);
+  }
   g.solve_cluster = cfg.solve_cluster > 0 ? cfg.solve_cluster : 16;
   g.solve_threads = cfg.solve_threads > 0 ? cfg.solve_threads : 512;
   if (g.solve_cluster > 16 || g.solve_threads < 32 || g.solve_threads > 1024 || g.solve_threads % 32) {

@@ -17,6 +17,7 @@
 #include "kernels.h"
 #include "cheb.h"
 #include "mg.h"
+#include "poisson.h"
 
 namespace pl {
 
@@ -498,6 +499,86 @@ void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   }  // the Chebyshev path solved this system in the pressure launch; only its fallback is left here
   SolveArgs a{P.rhs, P.qc, 1e-4, 80, 1, 0, (mg || cheb) ? 1 : 0};
   k_pcg<<<1, SOLVER_THREADS, 0, st>>>(g, P, W, a);
+}
+
+// ---------------------------------------------------------------- grid-scale solves (dense box)
+
+// The liquid system in the power-of-two box: FLUID where the cell is on the liquid list, the grid's
+// AIR / SOLID elsewhere, SOLID outside the grid (so the box operator is the liquid list's operator:
+// diagonal = non-SOLID neighbours, -1 between liquid neighbours); b = rhs on the liquid cells (0 on an
+// inactive substep, which the solve then finishes at once).
+__global__ void k_box_embed(Geo g, DevPtrs P, const double* rhs, int with_cells) {
+  const long long nb = (long long)g.bx * g.by * g.bz;
+  const bool act = P.sc->active != 0;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nb; v += (long long)gridDim.x * blockDim.x) {
+    const int i = int(v % g.bx), j = int((v / g.bx) % g.by), k = int(v / ((long long)g.bx * g.by));
+    uint8_t t = SOLID;
+    float b = 0.f;
+    if (i < g.nx && j < g.ny && k < g.nz) {
+      const int c = i + g.nx * (j + g.ny * k);
+      const int li = P.lidx[c];
+      if (li >= 0) {
+        t = FLUID;
+        if (act) b = float(rhs[li]);
+      } else {
+        t = P.cell[c] == SOLID ? SOLID : AIR;
+      }
+    }
+    if (with_cells) P.box_cell[v] = t;
+    P.box_b[v] = b;
+  }
+}
+
+// The box solution back on the liquid list, and the solve's outcome into the scalar block (the
+// pressure solve counts a failure when it did not converge, solver3d.ts:540).
+__global__ void k_box_finish(Geo g, DevPtrs P, double* q, int correction) {
+  SimScalars* sc = P.sc;
+  if (!sc->active) return;
+  const int m = sc->m;
+  const int nxy = g.nx * g.ny;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int c = P.list[t];
+    const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / nxy;
+    q[t] = P.box_x[i + (long long)g.bx * (j + (long long)g.by * k)];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int it = int(P.box_out[0]);
+    const double res = P.box_out[2];
+    if (correction) {
+      sc->corr_iters = it;
+      sc->corr_residual = res;
+    } else {
+      sc->last_iters = it;
+      sc->last_residual = res;
+      if (P.box_out[1] == 0) sc->failures++;
+    }
+  }
+}
+
+static unsigned box_blocks(const Geo& g) {
+  const long long nb = (long long)g.bx * g.by * g.bz;
+  return unsigned(std::min<long long>((nb + 255) / 256, 148 * 16));
+}
+
+int launch_box_pressure(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen) {
+  SolverWs W = ws_of(P, g.nc);
+  k_solve_setup<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, W, 1, 0);
+  k_box_embed<<<box_blocks(g), 256, 0, st>>>(g, P, W.bp, 1);
+  int rc = poisson_capture_setup(box, P.box_cell, st, err, errlen);
+  if (!rc) rc = poisson_capture_solve(box, P.box_b, P.box_x, g.tol, g.max_iter, st, err, errlen);
+  if (rc) return rc;
+  poisson_capture_result(box, P.box_out, st);
+  k_box_finish<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, P.q, 0);
+  return PL_OK;
+}
+
+int launch_box_correction(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen) {
+  k_box_embed<<<box_blocks(g), 256, 0, st>>>(g, P, P.rhs, 0);
+  int rc = poisson_capture_solve(box, P.box_b, P.box_x, 1e-4, 80, st, err, errlen);  // solver3d.ts:673
+  if (rc) return rc;
+  poisson_capture_result(box, P.box_out, st);
+  k_box_finish<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, P.qc, 1);
+  return PL_OK;
 }
 
 // ---------------------------------------------------------------- standalone solve

@@ -30,7 +30,7 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_unet_set_loss",
+    "pl_unet_set_loss", "pl_set_unet",
     "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
@@ -106,6 +106,7 @@ def lib() -> C.CDLL:
     L.pl_unet_destroy.argtypes = [P]
     L.pl_unet_destroy.restype = None
     L.pl_unet_set_loss.argtypes = [P, C.c_int32]
+    L.pl_set_unet.argtypes = [P, P]
     L.pl_get_affine.argtypes = [P, fp]
     L.pl_set_affine.argtypes = [P, fp]
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
@@ -340,6 +341,11 @@ class Simulation3D:
             c = np.broadcast_to(c, (self.n, 3, 3))
         c = np.ascontiguousarray(c).reshape(-1)
         _check(lib().pl_set_affine(self.handle, _ptr(c, C.c_float)))
+
+    def set_unet(self, net: "UNet"):
+        """pl_set_unet: the network of a PRECOND_LEARNED simulation (kept alive by this object)."""
+        _check(lib().pl_set_unet(self.handle, net._h))
+        self._net = net
 
     def field(self, which: int) -> np.ndarray:
         n = self.nfaces if which in abi.FACE_FIELDS else self.nc

@@ -39,14 +39,16 @@ def apply_a(cell: np.ndarray, x: np.ndarray) -> np.ndarray:
 
 
 def harvest_pour_systems(cell_mm: float = 5.0, count: int = 32, every: int = 12, seconds: float = 12.0,
-                         preconditioner: int = abi.PRECOND_CHEB, box: tuple | None = None):
-    """Run the gentle pour on the engine and collect `count` pressure systems, one every `every` substeps.
+                         preconditioner: int = abi.PRECOND_CHEB, box: tuple | None = None, **over):
+    """Run the gentle pour on the engine and collect `count` pressure systems, one every `every` substeps
+    (keyword overrides of the config by field name, e.g. domain, transfer, solve_precision).
 
     Returns (box (nx, ny, nz), cells u8 (count, cells), r f32, e f32): r = A e with e the engine's
     pressure on the liquid cells."""
-    cfg = abi.gentle_pour(cell_mm, seconds)
+    cfg = abi.gentle_pour(cell_mm, seconds, **over)
     cfg.preconditioner = preconditioner
-    cfg.solve_precision = abi.SOLVE_F64
+    if "solve_precision" not in over:
+        cfg.solve_precision = abi.SOLVE_MIXED if preconditioner == abi.PRECOND_BOX_MG else abi.SOLVE_F64
     sim = E.Simulation3D(cfg)
     box = box or box_for(sim.nx, sim.ny, sim.nz)
     X, Y, Z = box
