@@ -59,6 +59,13 @@ def parse():
     ap.add_argument("--poisson-n", type=int, default=128, help="grid of the isolated Poisson batch (0: skip it)")
     ap.add_argument("--poisson-count", type=int, default=64, help="snapshots of the isolated Poisson batch per GPU")
     ap.add_argument("--poisson-cpu-sample", type=int, default=4, help="snapshots the CPU oracle solves as its sample")
+    ap.add_argument("--full-mm", type=float, default=2.5,
+                    help="cell size of the full-domain APIC pour on the grid-scale solves (0: skip it)")
+    ap.add_argument("--full-start", type=float, default=1.5, help="simulated seconds before its timed substeps")
+    ap.add_argument("--full-steps", type=int, default=100, help="its timed substeps (grid-scale multigrid PCG)")
+    ap.add_argument("--learned-train-s", type=float, default=45.0,
+                    help="seconds of network training for its learned-PCG leg (0: skip the leg)")
+    ap.add_argument("--learned-steps", type=int, default=10, help="timed substeps of the learned-PCG leg")
     return ap.parse_args()
 
 
@@ -296,6 +303,88 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
     return out
 
 
+def run_full_domain(args, world: int, rank: int) -> dict | None:
+    """The full-domain APIC pour (both halves of the pot; at 2.5 mm 126 x 126 x 64 cells and 752,630
+    parcels) on the grid-scale pressure solves: multigrid PCG, then learned flexible CG (network trained
+    here on residual/correction pairs of the same pour, multigrid fall-back) from the same state. Both end
+    every solve on the reference's max-norm 1e-6 rule; device time from the substep graph's stage events."""
+    if args.full_mm <= 0:
+        return None
+    import torch
+
+    import teapotfluidsimulation_b200 as pkg
+    from teapotfluidsimulation_b200 import abi
+    from teapotfluidsimulation_b200 import engine as E
+    from teapotfluidsimulation_b200 import learned as Lr
+
+    def make(pre):
+        cfg = abi.gentle_pour(args.full_mm, 20, domain=abi.DOMAIN_FULL, transfer=abi.TRANSFER_APIC)
+        cfg.preconditioner = pre
+        cfg.solve_precision = abi.SOLVE_MIXED
+        cfg.device = torch.cuda.current_device()
+        return pkg.Simulation3D(cfg)
+
+    def timed(sim, k):
+        sim.enable_stage_timing(True)
+        acc, its, cits = {}, [], []
+        d0 = sim.diagnostics()
+        for _ in range(k):
+            sim.enqueue(1)
+            sim.sync()
+            for name, v in sim.stage_times().items():
+                acc[name] = acc.get(name, 0.0) + v
+            d = sim.diagnostics()
+            its.append(d["pressureIterations"])
+            cits.append(d["correctionIterations"])
+        d1 = sim.diagnostics()
+        ms = allmax(sum(acc.values()), world)
+        return {"substeps": k, "ms_per_substep": ms / k,
+                "sim_s_per_wall_s": allsum(d1["time"] - d0["time"], world) / (ms / 1e3),
+                "pressure_ms_per_substep": acc["pressure"] / k, "correction_ms_per_substep": acc["correction"] / k,
+                "pressure_iterations_mean": float(np.mean(its)), "correction_iterations_mean": float(np.mean(cits)),
+                "pressure_failures": d1["pressureFailures"] - d0["pressureFailures"],
+                "stages_ms_per_substep": {name: v / k for name, v in acc.items()}}
+
+    mg = make(abi.PRECOND_BOX_MG)
+    mg.advance(args.full_start)
+    out = {"workload": f"gentle pour at {args.full_mm} mm, full domain (no symmetry plane), APIC, "
+                       f"timed from t = {args.full_start} s; the liquid system embedded in a power-of-two box",
+           "parcels": mg.n, "grid": [mg.nx, mg.ny, mg.nz], "liquid_cells": mg.diagnostics()["liquidCells"]}
+    out["mg"] = timed(mg, args.full_steps)
+    if args.learned_train_s > 0:
+        t0 = time.perf_counter()
+        box, cells, r, e = Lr.harvest_pour_systems(cell_mm=args.full_mm, count=12, every=25, seconds=20.0,
+                                                   preconditioner=abi.PRECOND_BOX_MG, domain=abi.DOMAIN_FULL,
+                                                   transfer=abi.TRANSFER_APIC)
+        tc, tr, te = Lr.residual_pairs(box, cells, r, e, iters=(1, 2, 4))
+        harvest_s = time.perf_counter() - t0
+        npairs = int(tc.shape[0])
+        del cells, r, e
+        net = E.UNet(seed=2)
+        net.set_loss(E.UNET_LOSS_ENERGY)
+        t0 = time.perf_counter()
+        hist = Lr.train(net, box, tc, tr, te, steps=1_000_000, batch=2, lr=1e-3, time_limit=args.learned_train_s)
+        train_s = time.perf_counter() - t0
+        del tc, tr, te
+        ln = make(abi.PRECOND_LEARNED)
+        ln.set_unet(net)
+        ln.set_state(mg.get_state(), mg.particles())
+        ln.set_affine(mg.affine())
+        mg_again = timed(mg, args.learned_steps)  # the same stretch of the pour with multigrid
+        ln_res = timed(ln, args.learned_steps)
+        ln_res["training"] = {"pairs": npairs, "box": list(box), "steps": len(hist), "seconds": train_s,
+                              "harvest_and_pairs_s": harvest_s, "loss_first": hist[0],
+                              "loss_last20": float(np.mean(hist[-20:])), "loss": "energy norm",
+                              "pairs_from": "12 pressure systems of the same pour and MG-PCG iterates 1, 2, 4"}
+        out["learned"] = ln_res
+        out["mg_same_stretch"] = mg_again
+        out["learned_over_mg_pressure_time"] = ln_res["pressure_ms_per_substep"] / mg_again["pressure_ms_per_substep"]
+        ln.destroy()
+        net.destroy()
+    mg.destroy()
+    return out
+
+
 def run_cpu_baseline(args, substeps: int) -> dict:
     """The CPU FP64 restatement of the reference solver on a bounded sample of the same workload."""
     from oracle import oracle as O
@@ -457,11 +546,14 @@ def run_ours(args):
     }
     if clk:
         line["clocks"] = clk
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
         line["cpu_baseline"] = run_cpu_baseline(args, args.cpu_sample)
     pois = run_poisson(args, world, rank)
     if pois is not None:
         line["poisson_batch"] = pois
+    full = run_full_domain(args, world, rank)
+    if full is not None:
+        line["full_domain"] = full
     if rank == 0:
         print(json.dumps(line))
     e2e_sim.destroy()

@@ -1118,7 +1118,9 @@ struct PoissonT : PoissonImpl {
   // r = b, x = 0, p = p1 = 0 and the per-snapshot state (enqueued on s0, capturable).
   void start(const float* b, double* x, double tol, int max_iter, cudaStream_t s0) {
     const TG& G = L[0].G;
-    cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);  // inactive tiles' partials stay 0
+    // inactive tiles' partials stay 0 (tiles active in an earlier solve on other cells are not rewritten)
+    cudaMemsetAsync(part, 0, size_t(count) * G.ntile * 8, s0);
+    if (learned()) cudaMemsetAsync(part2, 0, size_t(count) * G.ntile * 8, s0);
     cudaMemsetAsync(x, 0, size_t(count) * G.nc * 8, s0);
     cudaMemsetAsync(p1, 0, size_t(count) * G.nc * sizeof(T), s0);
     if (learned()) cudaMemsetAsync(rold, 0, size_t(count) * G.nc * sizeof(T), s0);

@@ -90,3 +90,32 @@ def test_history_records_the_residuals(trained, engine):
     for i, (q, n) in enumerate(zip(h, it)):
         assert q[0].size == n and q[1] == 0
         assert q[0][-1] <= 1e-6 * np.abs(r[i]).max() * 10
+
+
+def test_reused_solver_matches_a_fresh_one(trained, engine):
+    # a solver object that first solved other systems (another active-tile footprint) gives the same
+    # iterations and bitwise the same solution as a fresh one: no per-tile state survives a solve
+    Lr, box, cells, r, e, net, hist = trained
+    E = engine.engine
+    X, Y, Z = box
+    n = X * Y * Z
+
+    def run(pb, c, b):
+        dc, db = torch.from_numpy(c.copy()).cuda(), torch.from_numpy(b.copy()).cuda()
+        dx = torch.zeros((c.shape[0], n), dtype=torch.float64, device="cuda")
+        it, res, conv = pb.solve(dc.data_ptr(), db.data_ptr(), dx.data_ptr(), 1e-6, 400)
+        return it, dx.cpu().numpy()
+
+    reduced = cells[:2].copy()  # the lower half's liquid turned to air: tiles active before are inactive now
+    low = reduced[:, : n // 2]
+    low[(low & 3) == 1] = 0
+    pb = E.PoissonBatch(box, 2, E.POISSON_LEARNED, 1)
+    E._check(E.lib().pl_poisson_set_unet(pb._h, net._h))
+    run(pb, cells[:2], r[:2])
+    it_a, x_a = run(pb, reduced, r[:2])
+    pb.destroy()
+    pb = E.PoissonBatch(box, 2, E.POISSON_LEARNED, 1)
+    E._check(E.lib().pl_poisson_set_unet(pb._h, net._h))
+    it_b, x_b = run(pb, reduced, r[:2])
+    pb.destroy()
+    assert np.array_equal(it_a, it_b) and np.array_equal(x_a, x_b)
