@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--learned-train-s", type=float, default=45.0,
                     help="seconds of network training for its learned-PCG leg (0: skip the leg)")
     ap.add_argument("--learned-steps", type=int, default=10, help="timed substeps of the learned-PCG leg")
+    ap.add_argument("--ensemble-count", type=int, default=256, help="pours of the seeded ensemble (0: skip it)")
+    ap.add_argument("--ensemble-mm", type=float, default=5.0, help="cell size of the ensemble's pours")
+    ap.add_argument("--ensemble-steps", type=int, default=40, help="timed substeps per pour of the ensemble")
     return ap.parse_args()
 
 
@@ -303,6 +306,42 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
     return out
 
 
+UNET_FLOP_PER_CELL = 2 * 27 * (  # the 11 convolutions as computed (channels padded to 16), per fine cell
+    (16 * 16 + 16 * 16 + 48 * 16 + 16 * 16 + 16 * 16)  # full resolution
+    + (16 * 32 + 32 * 32 + 96 * 32 + 32 * 32) / 8  # half
+    + (32 * 64 + 64 * 64) / 64)  # quarter
+
+
+def unet_throughput(net, box, pairs) -> dict:
+    """The network's forward pass (the preconditioner application: BF16 tensor-core convolutions) on two
+    boxes, CUDA-event timed, as FLOP/s against the measured dense BF16 peak."""
+    import torch
+
+    X, Y, Z = box
+    dc = torch.from_numpy(np.ascontiguousarray(pairs[0])).cuda()
+    dr = torch.from_numpy(np.ascontiguousarray(pairs[1])).cuda()
+    dz = torch.zeros_like(dr)
+    count = dc.shape[0]
+    for _ in range(2):
+        net.apply(dc.data_ptr(), dr.data_ptr(), dz.data_ptr(), X, Y, Z, count)
+    reps = 5
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.apply(dc.data_ptr(), dr.data_ptr(), dz.data_ptr(), X, Y, Z, count)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flop = UNET_FLOP_PER_CELL * X * Y * Z * count
+    peaks, kind = measured_peaks()
+    tf = flop / (ms / 1e3) / 1e12
+    return {"boxes": count, "box": [X, Y, Z], "ms_per_apply": ms, "gflop_per_apply": flop / 1e9,
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peaks.get("bf16_tflops"), "unit": "TFLOP/s",
+                         "frac": tf / peaks.get("bf16_tflops", 1.0), "peak_kind": kind},
+            "kernels": "k_conv: implicit-GEMM 3x3x3 convolutions, BF16 mma.sync m16n8k16, FP32 accumulation"}
+
+
 def run_full_domain(args, world: int, rank: int) -> dict | None:
     """The full-domain APIC pour (both halves of the pot; at 2.5 mm 126 x 126 x 64 cells and 752,630
     parcels) on the grid-scale pressure solves: multigrid PCG, then learned flexible CG (network trained
@@ -359,6 +398,7 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
         tc, tr, te = Lr.residual_pairs(box, cells, r, e, iters=(1, 2, 4))
         harvest_s = time.perf_counter() - t0
         npairs = int(tc.shape[0])
+        cells_for_timing = (tc[:2].copy(), tr[:2].copy())
         del cells, r, e
         net = E.UNet(seed=2)
         net.set_loss(E.UNET_LOSS_ENERGY)
@@ -366,6 +406,8 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
         hist = Lr.train(net, box, tc, tr, te, steps=1_000_000, batch=2, lr=1e-3, time_limit=args.learned_train_s)
         train_s = time.perf_counter() - t0
         del tc, tr, te
+        out["unet_conv"] = unet_throughput(net, box, cells_for_timing)
+        del cells_for_timing
         ln = make(abi.PRECOND_LEARNED)
         ln.set_unet(net)
         ln.set_state(mg.get_state(), mg.particles())
@@ -383,6 +425,63 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
         net.destroy()
     mg.destroy()
     return out
+
+
+def run_ensemble(args, world: int, rank: int) -> dict | None:
+    """A seeded ensemble of pours (fill U[0.6, 1.0] L, peak tilt U[60, 110] deg, tilt-in ramp U[4, 12] s;
+    uneven grids), sharded round-robin over the ranks, each pour on its own stream with the substeps of all
+    pours interleaved; timed by the host clock around the whole set (every pour's stream synchronised),
+    against the same pours run one after another."""
+    if args.ensemble_count <= 0:
+        return None
+    import torch
+
+    from teapotfluidsimulation_b200 import abi
+    from teapotfluidsimulation_b200 import engine as E
+
+    cfgs = E.ensemble_configs(2026, args.ensemble_count, args.ensemble_mm, 20.0)
+    mine = cfgs[rank::world]
+    for c in mine:
+        c.preconditioner = abi.PRECOND_CHEB
+        c.solve_precision = abi.SOLVE_MIXED
+        c.device = torch.cuda.current_device()
+    t0 = time.perf_counter()
+    ens = E.Ensemble(mine)
+    create_s = time.perf_counter() - t0
+    grids = [m.nx * m.ny * m.nz for m in ens.members]
+    parcels = sum(m.n for m in ens.members)
+    ens.advance(0.6)  # past the start delay, into the tilt
+    ens.enqueue(3)
+    t_before = [m.diagnostics()["time"] for m in ens.members]
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.enqueue(args.ensemble_steps)
+    torch.cuda.synchronize()
+    wall = allmax(time.perf_counter() - t0, world)
+    sim_s = sum(m.diagnostics()["time"] - t for m, t in zip(ens.members, t_before))
+    fails = sum(m.diagnostics()["pressureFailures"] for m in ens.members)
+    # the same kind of work one pour at a time (the first few pours), for the concurrency gain
+    seq_wall, seq_sim = 0.0, 0.0
+    for m in ens.members[: min(8, len(ens.members))]:
+        t = m.diagnostics()["time"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.enqueue(args.ensemble_steps)
+        m.sync()
+        seq_wall += time.perf_counter() - t0
+        seq_sim += m.diagnostics()["time"] - t
+    ens.destroy()
+    total_sim = allsum(sim_s, world)
+    return {"workload": f"{args.ensemble_count} seeded gentle pours at {args.ensemble_mm} mm (half pot), "
+                        f"{args.ensemble_steps} substeps each from t = 0.6 s, Chebyshev cluster solves",
+            "pours": args.ensemble_count, "pours_per_gpu": len(mine), "parcels_per_gpu": parcels,
+            "cells_min": min(grids), "cells_max": max(grids), "create_s": create_s,
+            "sim_s_per_wall_s": total_sim / wall, "pour_substeps_per_s": allsum(len(mine), world) * args.ensemble_steps / wall,
+            "wall_s": wall, "pressure_failures": fails,
+            "one_at_a_time_sim_s_per_wall_s": seq_sim / seq_wall if seq_wall > 0 else None,
+            "concurrency_gain": (sim_s / wall) / (seq_sim / seq_wall) if seq_wall > 0 and seq_sim > 0 else None,
+            "timing": "host clock around the interleaved launches and every pour's synchronisation"}
 
 
 def run_cpu_baseline(args, substeps: int) -> dict:
@@ -554,6 +653,9 @@ def run_ours(args):
     full = run_full_domain(args, world, rank)
     if full is not None:
         line["full_domain"] = full
+    ens = run_ensemble(args, world, rank)
+    if ens is not None:
+        line["ensemble"] = ens
     if rank == 0:
         print(json.dumps(line))
     e2e_sim.destroy()

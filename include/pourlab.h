@@ -462,6 +462,28 @@ void pl_unet_destroy(pl_unet* u);
  * the caller keeps it alive while the simulation uses it). Rebuilds the substep graph. */
 int pl_set_unet(pl_sim* sim, pl_unet* u);
 
+/* ------------------------------------------------------------------ ensembles */
+
+/* Seeded pour configurations (no counterpart in the reference): count gentle pours at cell_mm, each
+ * lasting `seconds`, drawn from a mulberry32 stream (src/sim/rng.ts) seeded with `seed`: fill
+ * U[0.6, 1.0] L, peak tilt (motion.max_angle_deg) U[60, 110] degrees, tilt-in ramp
+ * (motion.tilt_duration) U[4, 12] s; pour i gets seed + 1 + i as its seeding seed. The grid of each
+ * follows from its fill and peak tilt (solver3d.ts:125-157), so an ensemble's grids are uneven. */
+int pl_ensemble_configs(uint32_t seed, int32_t count, double cell_mm, double seconds, pl_config* out);
+/* Many pours on one device: each pour a pl_sim with its own stream and substep graph; the calls below
+ * launch the pours' substeps interleaved, so their small kernels run concurrently, with one host
+ * synchronisation per pour per chunk. */
+typedef struct pl_ensemble pl_ensemble;
+int pl_ensemble_create(const pl_config* cfgs, int32_t count, pl_ensemble** out);
+int32_t pl_ensemble_size(const pl_ensemble* e);
+/* Member i (owned by the ensemble; every pl_* call on a pl_sim works on it). */
+pl_sim* pl_ensemble_member(pl_ensemble* e, int32_t i);
+/* Every pour advances by `duration` simulated seconds (advance(), solver3d.ts:281-286, per pour). */
+int pl_ensemble_advance(pl_ensemble* e, double duration);
+/* Every pour runs `substeps` stable substeps (those past its duration are no-ops). */
+int pl_ensemble_enqueue(pl_ensemble* e, int32_t substeps);
+void pl_ensemble_destroy(pl_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1128,4 +1128,122 @@ void pl_unet_destroy(pl_unet* u) {
   delete u;
 }
 
+// ------------------------------------------------------------------ ensembles
+
+int pl_ensemble_configs(uint32_t seed, int32_t count, double cell_mm, double seconds, pl_config* out) {
+  if (!out || count < 1 || !(cell_mm > 0) || !(seconds > 0)) return fail(PL_E_ARG, "pl_ensemble_configs: bad argument");
+  uint32_t a = seed;
+  auto next = [&]() {  // mulberry32 (src/sim/rng.ts:5-14)
+    a += 0x6d2b79f5u;
+    uint32_t t = a;
+    t = (t ^ (t >> 15)) * (t | 1u);
+    t ^= t + (t ^ (t >> 7)) * (t | 61u);
+    return double(t ^ (t >> 14)) / 4294967296.0;
+  };
+  for (int i = 0; i < count; i++) {
+    pl_config& c = out[i];
+    pl_gentle_pour(cell_mm, seconds, &c);
+    c.initial_volume = (0.6 + 0.4 * next()) * 1e-3;  // fill U[0.6, 1.0] L
+    c.motion.max_angle_deg = 60 + 50 * next();      // peak tilt U[60, 110] degrees
+    c.motion.tilt_duration = 4 + 8 * next();        // tilt-in ramp U[4, 12] s
+    c.seed = seed + 1 + uint32_t(i);
+  }
+  return PL_OK;
+}
+
+struct pl_ensemble {
+  std::vector<pl_sim*> sims;
+};
+
+void pl_ensemble_destroy(pl_ensemble* e) {
+  if (!e) return;
+  for (pl_sim* s : e->sims) pl_destroy(s);
+  delete e;
+}
+
+int pl_ensemble_create(const pl_config* cfgs, int32_t count, pl_ensemble** out) {
+  if (!cfgs || count < 1 || !out) return fail(PL_E_ARG, "pl_ensemble_create: bad argument");
+  *out = nullptr;
+  pl_ensemble* e = new pl_ensemble();
+  for (int i = 0; i < count; i++) {
+    pl_sim* s = nullptr;
+    const int rc = pl_create(&cfgs[i], &s);
+    if (rc) {
+      const std::string msg = g_err;
+      pl_ensemble_destroy(e);
+      return fail(rc, "pl_ensemble_create: pour %d: %s", i, msg.c_str());
+    }
+    e->sims.push_back(s);
+  }
+  *out = e;
+  return PL_OK;
+}
+
+int32_t pl_ensemble_size(const pl_ensemble* e) { return e ? int32_t(e->sims.size()) : 0; }
+
+pl_sim* pl_ensemble_member(pl_ensemble* e, int32_t i) {
+  return e && i >= 0 && i < int32_t(e->sims.size()) ? e->sims[i] : nullptr;
+}
+
+int pl_ensemble_enqueue(pl_ensemble* e, int32_t substeps) {
+  if (!e || substeps < 0) return fail(PL_E_ARG, "pl_ensemble_enqueue: bad argument");
+  for (pl_sim* s : e->sims) {  // control fields as pl_enqueue_substeps sets them
+    if (!s->exec) return fail(PL_E_STATE, "pl_ensemble_enqueue: a pour has no substep graph");
+    cudaSetDevice(s->device);
+    int rc = settle(s);
+    if (rc) return rc;
+    s->hs.end_time = INFINITY;
+    s->hs.force_step = 0;
+    std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
+    const size_t off = offsetof(SimScalars, end_time);
+    const size_t len = offsetof(SimScalars, active) - off;
+    CK(cudaMemcpyAsync((char*)s->P.sc + off, (char*)s->pinned + off, len, cudaMemcpyHostToDevice, s->st));
+  }
+  for (int k = 0; k < substeps; k++)  // interleaved: every pour's next substep before anyone's following one
+    for (pl_sim* s : e->sims) CK(cudaGraphLaunch(s->exec, s->st));
+  for (pl_sim* s : e->sims) {
+    const int rc = pull_scalars(s);
+    if (rc) return rc;
+  }
+  return PL_OK;
+}
+
+int pl_ensemble_advance(pl_ensemble* e, double duration) {
+  if (!e || !(duration >= 0)) return fail(PL_E_ARG, "pl_ensemble_advance: bad argument");
+  std::vector<double> end(e->sims.size());
+  for (size_t i = 0; i < e->sims.size(); i++) {
+    pl_sim* s = e->sims[i];
+    if (!s->exec) return fail(PL_E_STATE, "pl_ensemble_advance: a pour has no substep graph");
+    cudaSetDevice(s->device);
+    int rc = settle(s);
+    if (rc) return rc;
+    end[i] = s->hs.time + duration;  // solver3d.ts:282, per pour
+    s->hs.end_time = end[i];
+    s->hs.force_step = 0;
+    rc = push_scalars(s);
+    if (rc) return rc;
+  }
+  for (int guard = 0; guard < 1000000; guard++) {
+    std::vector<long> k(e->sims.size(), 0);
+    long kmax = 0;
+    for (size_t i = 0; i < e->sims.size(); i++) {
+      const pl_sim* s = e->sims[i];
+      if (!(s->hs.time < end[i] - 1e-12 && !host_finished(s))) continue;
+      const double remaining = std::min(end[i], s->g.duration) - s->hs.time;
+      k[i] = std::max(1L, std::min((long)std::ceil(remaining / host_stable_dt(s) * 1.05) + 1, 256L));
+      kmax = std::max(kmax, k[i]);
+    }
+    if (kmax == 0) break;
+    for (long q = 0; q < kmax; q++)  // interleaved launches on the pours' own streams
+      for (size_t i = 0; i < e->sims.size(); i++)
+        if (q < k[i]) CK(cudaGraphLaunch(e->sims[i]->exec, e->sims[i]->st));
+    for (size_t i = 0; i < e->sims.size(); i++)
+      if (k[i]) {
+        const int rc = pull_scalars(e->sims[i]);
+        if (rc) return rc;
+      }
+  }
+  return PL_OK;
+}
+
 }  // extern "C"

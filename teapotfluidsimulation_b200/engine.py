@@ -30,7 +30,8 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_unet_set_loss", "pl_set_unet",
+    "pl_unet_set_loss", "pl_set_unet", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
+    "pl_ensemble_member", "pl_ensemble_advance", "pl_ensemble_enqueue", "pl_ensemble_destroy",
     "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
@@ -107,6 +108,16 @@ def lib() -> C.CDLL:
     L.pl_unet_destroy.restype = None
     L.pl_unet_set_loss.argtypes = [P, C.c_int32]
     L.pl_set_unet.argtypes = [P, P]
+    L.pl_ensemble_configs.argtypes = [C.c_uint32, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.Config)]
+    L.pl_ensemble_create.argtypes = [C.POINTER(abi.Config), C.c_int32, C.POINTER(P)]
+    L.pl_ensemble_size.argtypes = [P]
+    L.pl_ensemble_size.restype = C.c_int32
+    L.pl_ensemble_member.argtypes = [P, C.c_int32]
+    L.pl_ensemble_member.restype = P
+    L.pl_ensemble_advance.argtypes = [P, C.c_double]
+    L.pl_ensemble_enqueue.argtypes = [P, C.c_int32]
+    L.pl_ensemble_destroy.argtypes = [P]
+    L.pl_ensemble_destroy.restype = None
     L.pl_get_affine.argtypes = [P, fp]
     L.pl_set_affine.argtypes = [P, fp]
     L.pl_poisson_generate.argtypes = [C.c_int32, C.c_int32, C.c_int32, u8p, fp, C.c_int32]
@@ -164,10 +175,14 @@ def autotune_solver(cfg: abi.Config, substeps: int = 3) -> tuple[int, int, float
 class Simulation3D:
     """The pour simulation on one B200 (the reference's Simulation3D / GpuSimulation3D surface)."""
 
-    def __init__(self, cfg: abi.Config):
+    def __init__(self, cfg: abi.Config, _member=None):
         L = lib()
         self._h = C.c_void_p()
-        _check(L.pl_create(C.byref(cfg), C.byref(self._h)))
+        self._owned = _member is None
+        if _member is None:
+            _check(L.pl_create(C.byref(cfg), C.byref(self._h)))
+        else:  # a pour of an Ensemble, which owns it
+            self._h = C.c_void_p(_member)
         self.cfg = cfg
         s = abi.Sizes()
         _check(L.pl_get_sizes(self._h, C.byref(s)))
@@ -183,7 +198,8 @@ class Simulation3D:
     def destroy(self):
         """GpuSimulation3D.destroy() (src/gpu3d/solver.ts:486-489)."""
         if self._h:
-            lib().pl_destroy(self._h)
+            if self._owned:
+                lib().pl_destroy(self._h)
             self._h = C.c_void_p()
 
     close = destroy
@@ -390,6 +406,47 @@ POISSON_MIC0 = 0
 POISSON_MG = 1
 POISSON_LEARNED = 2
 POISSON_PIN = 4
+
+
+def ensemble_configs(seed: int, count: int, cell_mm: float, seconds: float) -> list:
+    """pl_ensemble_configs: seeded gentle pours (fill U[0.6, 1.0] L, peak tilt U[60, 110] deg, tilt-in ramp
+    U[4, 12] s)."""
+    arr = (abi.Config * count)()
+    _check(lib().pl_ensemble_configs(seed, count, cell_mm, seconds, arr))
+    return list(arr)
+
+
+class Ensemble:
+    """Many pours on one device (pl_ensemble_*): each pour on its own stream, substeps interleaved."""
+
+    def __init__(self, cfgs: list):
+        arr = (abi.Config * len(cfgs))(*cfgs)
+        h = C.c_void_p()
+        _check(lib().pl_ensemble_create(arr, len(cfgs), C.byref(h)))
+        self._h = h
+        self.members = [Simulation3D(cfgs[i], _member=lib().pl_ensemble_member(h, i)) for i in range(len(cfgs))]
+
+    def __len__(self):
+        return len(self.members)
+
+    def advance(self, duration: float):
+        _check(lib().pl_ensemble_advance(self._h, duration))
+
+    def enqueue(self, substeps: int):
+        _check(lib().pl_ensemble_enqueue(self._h, substeps))
+
+    def destroy(self):
+        if self._h:
+            for m in self.members:
+                m.destroy()
+            lib().pl_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def poisson_generate(n: int, first: int, count: int, threads: int = 0) -> tuple[np.ndarray, np.ndarray]:
