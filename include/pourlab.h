@@ -445,6 +445,14 @@ int pl_unet_create(uint32_t seed, pl_unet** out);
  * which a preconditioner's quality decides CG's convergence. */
 enum pl_unet_loss { PL_UNET_LOSS_L2 = 0, PL_UNET_LOSS_ENERGY = 1 };
 int pl_unet_set_loss(pl_unet* u, int32_t kind);
+/* Convolution kernels: TCGEN05 (default; 5th-generation tensor cores, accumulator in tensor memory) or
+ * MMA_SYNC (the warp-level tensor-core path, kept for comparison). Both compute the same convolutions
+ * in BF16 with FP32 accumulation. */
+enum pl_unet_conv { PL_UNET_CONV_TCGEN05 = 0, PL_UNET_CONV_MMA_SYNC = 1 };
+int pl_unet_set_conv_kernel(pl_unet* u, int32_t kind);
+/* 1 if a tensor-core convolution of this network gave up a bounded wait (its output is then invalid),
+ * else 0. Synchronous. */
+int pl_unet_error(pl_unet* u);
 int32_t pl_unet_num_params(const pl_unet* u);
 int pl_unet_get_params(pl_unet* u, float* host);
 int pl_unet_set_params(pl_unet* u, const float* host); /* also resets the Adam moments */

@@ -1076,6 +1076,18 @@ int pl_unet_set_loss(pl_unet* u, int32_t kind) {
   return PL_OK;
 }
 
+int pl_unet_set_conv_kernel(pl_unet* u, int32_t kind) {
+  if (!u) return fail(PL_E_ARG, "pl_unet_set_conv_kernel: null argument");
+  if (pl::unet_set_conv_kernel(u->impl, kind)) return fail(PL_E_ARG, "pl_unet_set_conv_kernel: kind %d", kind);
+  return PL_OK;
+}
+
+int pl_unet_error(pl_unet* u) {
+  if (!u) return fail(PL_E_ARG, "pl_unet_error: null argument");
+  cudaSetDevice(u->device);
+  return pl::unet_error(u->impl);
+}
+
 int32_t pl_unet_num_params(const pl_unet* u) { return u ? pl::unet_nparams(u->impl) : 0; }
 
 int pl_unet_get_params(pl_unet* u, float* host) {

@@ -13,10 +13,12 @@
 //   out : 16->16 (channel 0 used)
 //
 // Kernels (NDHWC activations, x fastest among the cells, channels innermost):
-//  - k_conv: implicit GEMM out[v][n] = bias[n] + sum_t sum_k in[v + off_t][k] G[t][n][k] on the tensor
-//    cores (mma.sync m16n8k16, BF16 in, FP32 accumulate), one warp per 16 cells x all output
-//    channels; A and B fragments are loaded straight from the NDHWC tensor and the [tap][n][k] weights.
-//    The same kernel computes the data gradient with G[t][n][k] = W[26 - t][n][k] (flipped taps).
+//  - k_conv_tc (default): implicit GEMM out[v][n] = bias[n] + sum_t sum_k in[v + off_t][k] G[t][n][k]
+//    on the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 in, FP32 accumulator in tensor
+//    memory), 128 cells x all output channels per CTA, operands staged per tap in shared memory by
+//    asynchronous copies. k_conv computes the same on the warp-level tensor-core path (mma.sync
+//    m16n8k16, one warp per 16 cells), kept for comparison (pl_unet_set_conv_kernel). Both compute the
+//    data gradient with G[t][n][k] = W[26 - t][n][k] (flipped taps).
 //  - k_wgrad: weight gradient dW[t][ci][co] = sum_v in[v + off_t][ci] d[v][co] on the tensor cores:
 //    a CTA stages a chunk of cells of both operands transposed in shared memory ([channel][cell]) and
 //    accumulates the Cin x Cout tile; per-chunk partials are summed in a fixed order (deterministic).
@@ -147,6 +149,218 @@ __global__ void __launch_bounds__(128) k_conv(Box B, const bf16* __restrict__ in
       }
     }
   }
+}
+
+// ---------------------------------------------------------------- tcgen05 convolution (sm_100a)
+//
+// The same implicit GEMM on the 5th-generation tensor cores: one CTA of 128 threads per 128 output
+// cells (M = 128), all NOUT output channels (N), K = 27 taps x CIN in MMAs of K = 16. Per tap the CTA
+// stages the 128 gathered input rows (A: cells x CIN) and the tap's weights (B: NOUT x CIN) in shared
+// memory in the canonical K-major layout without swizzle (8-row x 16-byte core matrices; cores
+// adjacent in K 128 bytes apart, cores adjacent in M/N 256 bytes apart), then one thread issues the
+// tap's MMAs into an FP32 accumulator in tensor memory and commits them to the buffer's mbarrier.
+// Two buffers: the staging of tap t + 1 overlaps the MMAs of tap t. The epilogue reads the
+// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows of its cells).
+// Every mbarrier wait is bounded: on a timeout the CTA sets *err, stops issuing, waits (bounded) for
+// its MMAs in flight, frees its tensor memory and returns.
+
+constexpr int TC_SPIN = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (sm_100 format): start address, leading (K) and stride (M/N) byte
+// offsets, all in 16-byte units; descriptor version 1; no swizzle.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)((lbo & 0x3FFFF) >> 4) << 16) |
+         ((uint64_t)((sbo & 0x3FFFF) >> 4) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, N, M = 128.
+template <int N>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int i = 0; i < TC_SPIN; i++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int NOUT>
+__host__ __device__ constexpr int tc_cols() {
+  return NOUT <= 32 ? 32 : NOUT <= 64 ? 64 : 128;
+}
+
+constexpr int TC_STAGES = 4;  // (A, B) stages in flight: taps t + 1 .. t + 3 load while tap t multiplies
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+template <int NOUT>
+__global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__ in, int cin,
+                                                 const bf16* __restrict__ G, const float* __restrict__ bias, int relu,
+                                                 const bf16* __restrict__ mask, bf16* out_bf, float* out_f32,
+                                                 int* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  constexpr int NCOL = tc_cols<NOUT>();
+  constexpr uint32_t IDESC = tc_idesc<NOUT>();
+  constexpr int S = TC_STAGES;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int total = B.total();
+  const int v0 = blockIdx.x * 128;
+  const int a_bytes = 128 * cin * 2, b_bytes = NOUT * cin * 2;
+  const int stage_bytes = a_bytes + b_bytes;
+  const uint32_t sbase = smem_u32(smem);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + S);
+  if (tid == 0) {
+    for (int q = 0; q < S; q++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[q])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(NCOL)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const int v = v0 + tid;
+  const int kch = cin / 8;  // 16-byte chunks per row
+  // stage s <- tap t: this thread's gathered row (zero-filled outside the box) and its share of the
+  // tap's weights, as 16-byte asynchronous copies, one commit group per tap
+  auto load_tap = [&](int t, int s) {
+    const uint32_t a0 = sbase + s * stage_bytes, b0 = a0 + a_bytes;
+    const int nv = v < total ? tap_cell(B, v, t) : -1;
+    const bf16* src = nv >= 0 ? in + (size_t)nv * cin : in;
+    const uint32_t nbytes = nv >= 0 ? 16u : 0u;
+    const uint32_t arow = a0 + (tid >> 3) * 256 + (tid & 7) * 16;
+    for (int c = 0; c < kch; c++) cp_async16(arow + (c >> 1) * 4096 + (c & 1) * 128, src + 8 * c, nbytes);
+    const bf16* gt = G + (size_t)t * NOUT * cin;
+    for (int e = tid; e < NOUT * kch; e += 128) {
+      const int n = e / kch, c = e - n * kch;
+      cp_async16(b0 + (c >> 1) * (NOUT * 32) + ((n >> 3) * 2 + (c & 1)) * 128 + (n & 7) * 16,
+                 gt + (size_t)n * cin + 8 * c, 16u);
+    }
+  };
+  for (int p = 0; p < S - 1; p++) {
+    load_tap(p, p);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  bool bad = false;
+  bool timed_out = false;
+  int issued = 0;  // taps whose MMAs were issued
+  for (int t = 0; t < 27; t++) {
+    const int s = t % S;
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");  // this thread's copies of tap t landed
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");      // ... and are visible to the MMA
+    if (__syncthreads_or(bad ? 1 : 0)) {
+      timed_out = true;
+      break;
+    }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = sbase + s * stage_bytes, b0 = a0 + a_bytes;
+      for (int kc = 0; kc < cin / 16; kc++) {
+        const uint64_t ad = tc_desc(a0 + kc * 4096, 128, 256);
+        const uint64_t bd = tc_desc(b0 + kc * (NOUT * 32), 128, 256);
+        const uint32_t acc = (t | kc) != 0 ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[s]))
+                   : "memory");
+    }
+    issued = t + 1;
+    const int tn = t + S - 1;
+    if (tn < 27) {
+      const int sn = tn % S;  // = (t - 1) % S: free once the MMAs of tap t - 1 are done
+      if (t >= 1) bad = !tc_wait(&mbar[sn], uint32_t(((t - 1) / S) & 1));
+      if (!bad) load_tap(tn, sn);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");  // (empty past the last tap: keeps the count)
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  // the last commit tracks every MMA issued before it
+  bool done = true;
+  if (issued > 0) {
+    const int tl = issued - 1;
+    done = tc_wait(&mbar[tl % S], uint32_t((tl / S) & 1));
+  }
+  if (__syncthreads_or(done ? 0 : 1)) timed_out = true;
+  if (timed_out) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(lane_base + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int vr = v0 + warp * 32 + lane;
+      if (vr < total) {
+        float f[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+          float x = __uint_as_float(r[q]);
+          if (bias) x += bias[c0 + q];
+          if (relu) x = fmaxf(x, 0.f);
+          if (mask && !(__bfloat162float(mask[(size_t)vr * NOUT + c0 + q]) > 0.f)) x = 0.f;
+          f[q] = x;
+        }
+        if (out_f32) {
+          float4* o = reinterpret_cast<float4*>(out_f32 + (size_t)vr * NOUT + c0);
+#pragma unroll
+          for (int q = 0; q < 4; q++) o[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+        }
+        if (out_bf) {
+          __align__(16) bf16 h[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) h[q] = __float2bfloat16(f[q]);
+          uint4* o = reinterpret_cast<uint4*>(out_bf + (size_t)vr * NOUT + c0);
+          o[0] = *reinterpret_cast<uint4*>(&h[0]);
+          o[1] = *reinterpret_cast<uint4*>(&h[8]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+  }
+}
+
+// Dynamic shared memory of k_conv_tc: TC_STAGES (A, B) stages, the mbarriers and the TMEM address; at
+// least enough that no more CTAs share an SM than its 512 tensor-memory columns serve.
+inline size_t tc_smem(int cin, int nout) {
+  const size_t need = TC_STAGES * (size_t(128) * cin * 2 + size_t(nout) * cin * 2) + 8 * TC_STAGES + 64;
+  const int ncol = nout <= 32 ? 32 : nout <= 64 ? 64 : 128;
+  const size_t floor_b = size_t(233472) / size_t(512 / ncol) + 1024;
+  return std::max(need, ncol > 32 ? floor_b : need);
 }
 
 // Weight gradient of one tap t = blockIdx.y: part[chunk][t][ci][co] = sum over the CTA's cells v of
@@ -286,18 +500,21 @@ __global__ void k_pool_bwd_add(Box F, Box Cb, const bf16* dc, int c, bf16* dst) 
 // Nearest-neighbour upsampling of a (coarse, cu channels) into channels [0, cu) of a concatenation of
 // width ctot, and the skip tensor (fine, cs channels) into channels [cu, ctot).
 __global__ void k_up_concat(Box F, Box Cb, const bf16* coarse, int cu, const bf16* skip, int cs, bf16* out) {
-  const int ctot = cu + cs;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= F.total() * ctot) return;
-  const int ch = i % ctot, v = i / ctot;
+  const int ctot = cu + cs, q8 = ctot / 8;  // 16-byte chunks per output cell (channels are multiples of 16)
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)F.total() * q8) return;
+  const int q = int(i % q8), v = int(i / q8);
+  const int ch = q * 8;
+  uint4 val;
   if (ch >= cu) {
-    out[i] = skip[(size_t)v * cs + ch - cu];
-    return;
+    val = *reinterpret_cast<const uint4*>(skip + (size_t)v * cs + ch - cu);
+  } else {
+    const int per = F.cells(), s = v / per, cc = v % per;
+    const int x = cc % F.X, y = (cc / F.X) % F.Y, z = cc / (F.X * F.Y);
+    const int pv = s * Cb.cells() + ((z >> 1) * Cb.Y + (y >> 1)) * Cb.X + (x >> 1);
+    val = *reinterpret_cast<const uint4*>(coarse + (size_t)pv * cu + ch);
   }
-  const int per = F.cells(), s = v / per, cc = v % per;
-  const int x = cc % F.X, y = (cc / F.X) % F.Y, z = cc / (F.X * F.Y);
-  const int pv = s * Cb.cells() + ((z >> 1) * Cb.Y + (y >> 1)) * Cb.X + (x >> 1);
-  out[i] = coarse[(size_t)pv * cu + ch];
+  *reinterpret_cast<uint4*>(out + (size_t)v * ctot + ch) = val;
 }
 
 // Gradient of k_up_concat: the coarse part sums its 8 children (masked by the coarse activation's
@@ -333,31 +550,56 @@ __global__ void k_relu_mask(int n, bf16* d, const bf16* act) {
   if (!(__bfloat162float(act[i]) > 0.f)) d[i] = __float2bfloat16(0.f);
 }
 
-// Per-sample scale s = max |r| over the liquid cells and, with e, the target energy sum e^2.
-__global__ void k_sample_stats(Box B, const uint8_t* cell, const float* r, const float* e, float* scale,
-                               float* energy) {
-  const int s = blockIdx.x;
+// Per-sample scale s = max |r| over the liquid cells and, with e, the target energy sum e^2, in two
+// passes with a fixed order: STAT_BLOCKS blocks per sample write partials (each block a contiguous
+// range of the sample's cells, its threads folded in a fixed tree), then one thread per sample folds
+// them in block order.
+constexpr int STAT_BLOCKS = 256;
+
+__global__ void k_stats_part(Box B, const uint8_t* cell, const float* r, const float* e, float* pm, float* pe) {
+  const int s = blockIdx.y, b = blockIdx.x;
   const int per = B.cells();
+  const int chunk = (per + STAT_BLOCKS - 1) / STAT_BLOCKS;
+  const int c1 = min(per, (b + 1) * chunk);
   float m = 0.f, en = 0.f;
-  for (int c = threadIdx.x; c < per; c += blockDim.x) {
+  for (int c = b * chunk + threadIdx.x; c < c1; c += blockDim.x) {
     const int v = s * per + c;
     if ((cell[v] & 3) != FLUID) continue;
     m = fmaxf(m, fabsf(r[v]));
     if (e) en += e[v] * e[v];
   }
-  __shared__ float sm[256], se[256];
-  sm[threadIdx.x] = m;
-  se[threadIdx.x] = en;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    en += __shfl_xor_sync(0xffffffffu, en, o);
+  }
+  __shared__ float sm[32], se[32];
+  if ((threadIdx.x & 31) == 0) {
+    sm[threadIdx.x >> 5] = m;
+    se[threadIdx.x >> 5] = en;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    float a = 0.f, b = 0.f;
-    for (int q = 0; q < (int)blockDim.x; q++) {
-      a = fmaxf(a, sm[q]);
-      b += se[q];
+    float a = 0.f, c = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      a = fmaxf(a, sm[w]);
+      c += se[w];
     }
-    scale[s] = a > 0.f ? a : 1.f;
-    if (energy) energy[s] = b > 0.f ? b : 1.f;
+    pm[s * STAT_BLOCKS + b] = a;
+    pe[s * STAT_BLOCKS + b] = c;
   }
+}
+
+__global__ void k_stats_fin(int count, const float* pm, const float* pe, float* scale, float* energy) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  float a = 0.f, c = 0.f;
+  for (int b = 0; b < STAT_BLOCKS; b++) {
+    a = fmaxf(a, pm[s * STAT_BLOCKS + b]);
+    c += pe[s * STAT_BLOCKS + b];
+  }
+  scale[s] = a > 0.f ? a : 1.f;
+  if (energy) energy[s] = c > 0.f ? c : 1.f;
 }
 
 // Network input: [r / s, liquid, air, 0 ...] (16 channels).
@@ -537,9 +779,11 @@ struct UNetImpl {
   size_t ws_bytes = 0;
   bf16 *x0, *a0, *s1, *p1, *a2, *s2, *p2, *a4, *a5, *c2, *a6, *a7, *c1, *a8, *a9;  // forward
   bf16 *d_o, *d_a9, *d_a8, *d_c1, *d_a7, *d_a6, *d_c2, *d_a5, *d_a4, *d_p2, *d_s2, *d_a2, *d_p1, *d_s1, *d_a0;
-  float *o, *scale, *energy, *part, *loss_part, *loss, *ad;
+  float *o, *scale, *energy, *part, *loss_part, *loss, *ad, *stat_m, *stat_e;
   int nchunk = 0, nloss = 0;
   int loss_kind = 0;  // PL_UNET_LOSS_L2 or PL_UNET_LOSS_ENERGY
+  int conv_kernel = PL_UNET_CONV_TCGEN05;  // or PL_UNET_CONV_MMA_SYNC
+  int* dev_err = nullptr;  // set by a tcgen05 convolution whose bounded wait gave up
 
   ~UNetImpl() {
     if (wmem) cudaFree(wmem);
@@ -555,7 +799,7 @@ struct UNetImpl {
     }
     size_t bf = 0;
     for (int l = 0; l < NLAYER; l++) bf += 2 * size_t(27) * SPEC[l].cin * SPEC[l].cout;
-    const size_t total = size_t(nparam) * 4 * 4 + bf * 2 + 4096;
+    const size_t total = size_t(nparam) * 4 * 4 + bf * 2 + 4096 + 256;
     if (cudaMalloc(&wmem, total) != cudaSuccess) {
       snprintf(err, errlen, "pl_unet_create: cudaMalloc(%zu) failed", total);
       wmem = nullptr;
@@ -574,6 +818,13 @@ struct UNetImpl {
       gb[l] = q;
       q += size_t(27) * SPEC[l].cin * SPEC[l].cout;
     }
+    dev_err = reinterpret_cast<int*>(static_cast<char*>(wmem) + total - 256);
+    const int big = 227 * 1024;
+    cudaFuncSetAttribute(k_conv_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     // He initialisation from a fixed generator (mulberry32 + Box-Muller); real input channels only
     std::vector<float> h(nparam, 0.f);
     uint32_t a = seed;
@@ -620,7 +871,7 @@ struct UNetImpl {
     size_t bytes = 0;
     for (size_t s : sz) bytes += ((s * 2 + 255) & ~size_t(255));
     const size_t fbytes = n1 * 16 * 4 + 2 * size_t(count) * 4 + size_t(nchunk) * maxw * 4 + size_t(nloss) * 4 + 1024 +
-                          n1 * 4 + 256;
+                          n1 * 4 + 256 + 2 * size_t(count) * STAT_BLOCKS * 4 + 256;
     if (cudaMalloc(&ws, bytes + fbytes + 4096) != cudaSuccess) {
       ws = nullptr;
       snprintf(err, errlen, "pl_unet: workspace cudaMalloc(%zu) failed", bytes + fbytes);
@@ -650,6 +901,10 @@ struct UNetImpl {
     loss = (float*)p;
     p += 1024;
     ad = (float*)p;
+    p += n1 * 4;
+    p = (char*)(((uintptr_t)p + 255) & ~uintptr_t(255));
+    stat_m = (float*)p;
+    stat_e = stat_m + size_t(count) * STAT_BLOCKS;
     return PL_OK;
   }
 
@@ -663,6 +918,21 @@ struct UNetImpl {
   // out = conv_l(in) (forward, G = gf) or the data gradient (G = gb; then nout = cin of the layer).
   void conv(const Box& B, const bf16* in, int cin, const bf16* G, int nout, const float* bias, int relu,
             const bf16* mask, bf16* out_bf, float* out_f32, cudaStream_t st) {
+    if (conv_kernel == PL_UNET_CONV_TCGEN05) {
+      const unsigned blocks = nb(B.total(), 128);
+      const size_t sm = tc_smem(cin, nout);
+      if (nout == 16)
+        k_conv_tc<16><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else if (nout == 32)
+        k_conv_tc<32><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else if (nout == 48)
+        k_conv_tc<48><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else if (nout == 64)
+        k_conv_tc<64><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else
+        k_conv_tc<96><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      return;
+    }
     const long long warps = (B.total() + 15) / 16;
     const unsigned blocks = nb(warps * 32, 128);
     if (nout == 16)
@@ -679,7 +949,8 @@ struct UNetImpl {
 
   void forward(const uint8_t* cell, const float* r, cudaStream_t st) {
     prep_weights(st);
-    k_sample_stats<<<b1.count, 256, 0, st>>>(b1, cell, r, nullptr, scale, nullptr);
+    k_stats_part<<<dim3(STAT_BLOCKS, b1.count), 256, 0, st>>>(b1, cell, r, nullptr, stat_m, stat_e);
+    k_stats_fin<<<nb(b1.count, 128), 128, 0, st>>>(b1.count, stat_m, stat_e, scale, nullptr);
     k_pack_input<<<nb(b1.total(), 256), 256, 0, st>>>(b1, cell, r, scale, x0);
     auto L = [&](int l, const Box& B, const bf16* in, bf16* out, int relu, float* f32) {
       conv(B, in, SPEC[l].cin, gf[l], SPEC[l].cout, param + off_b[l], relu, nullptr, out, f32, st);
@@ -692,10 +963,10 @@ struct UNetImpl {
     k_pool<<<nb((long long)b3.total() * 32, 256), 256, 0, st>>>(b2, b3, s2, 32, p2);
     L(4, b3, p2, a4, 1, nullptr);
     L(5, b3, a4, a5, 1, nullptr);
-    k_up_concat<<<nb((long long)b2.total() * 96, 256), 256, 0, st>>>(b2, b3, a5, 64, s2, 32, c2);
+    k_up_concat<<<nb((long long)b2.total() * 96 / 8, 256), 256, 0, st>>>(b2, b3, a5, 64, s2, 32, c2);
     L(6, b2, c2, a6, 1, nullptr);
     L(7, b2, a6, a7, 1, nullptr);
-    k_up_concat<<<nb((long long)b1.total() * 48, 256), 256, 0, st>>>(b1, b2, a7, 32, s1, 16, c1);
+    k_up_concat<<<nb((long long)b1.total() * 48 / 8, 256), 256, 0, st>>>(b1, b2, a7, 32, s1, 16, c1);
     L(8, b1, c1, a8, 1, nullptr);
     L(9, b1, a8, a9, 1, nullptr);
     L(10, b1, a9, nullptr, 0, o);
@@ -761,7 +1032,8 @@ struct UNetImpl {
       k_sum<<<1, 32, 0, st>>>(loss_part, b1.count, loss);
       return;
     }
-    k_sample_stats<<<b1.count, 256, 0, st>>>(b1, cell, e, e, part, energy);  // energy of the targets
+    k_stats_part<<<dim3(STAT_BLOCKS, b1.count), 256, 0, st>>>(b1, cell, e, e, stat_m, stat_e);  // target energy
+    k_stats_fin<<<nb(b1.count, 128), 128, 0, st>>>(b1.count, stat_m, stat_e, part, energy);
     k_loss<<<nb(b1.total(), 256), 256, 0, st>>>(b1, cell, o, e, scale, energy, d_o, loss_part);
     k_sum<<<1, 32, 0, st>>>(loss_part, nloss, loss);
   }
@@ -843,7 +1115,9 @@ int unet_gradient(UNetImpl* u, const uint8_t* cell, const float* r, const float*
                                                1.f - std::pow(b1, float(u->adam_t)),
                                                1.f - std::pow(b2, float(u->adam_t)));
   }
+  int tc_err = 0;
   cudaError_t ce = cudaMemcpyAsync(loss, u->loss, 4, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(&tc_err, u->dev_err, 4, cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess && grad_host)
     ce = cudaMemcpyAsync(grad_host, u->grad, size_t(u->nparam) * 4, cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
@@ -851,7 +1125,23 @@ int unet_gradient(UNetImpl* u, const uint8_t* cell, const float* r, const float*
     snprintf(err, errlen, "pl_unet: %s", cudaGetErrorString(ce));
     return PL_E_CUDA;
   }
+  if (tc_err) {
+    snprintf(err, errlen, "pl_unet: a tensor-core convolution's bounded wait gave up");
+    return PL_E_TIMEOUT;
+  }
   return PL_OK;
+}
+
+int unet_set_conv_kernel(UNetImpl* u, int kind) {
+  if (kind != PL_UNET_CONV_TCGEN05 && kind != PL_UNET_CONV_MMA_SYNC) return PL_E_ARG;
+  u->conv_kernel = kind;
+  return PL_OK;
+}
+
+int unet_error(UNetImpl* u) {
+  int e = 0;
+  cudaMemcpy(&e, u->dev_err, 4, cudaMemcpyDeviceToHost);
+  return e;
 }
 
 }  // namespace pl

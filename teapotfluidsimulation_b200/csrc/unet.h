@@ -13,6 +13,8 @@ UNetImpl* unet_create(uint32_t seed, char* err, size_t errlen, int* rc);
 void unet_destroy(UNetImpl* u);
 int unet_nparams(const UNetImpl* u);
 void unet_set_loss(UNetImpl* u, int kind);
+int unet_set_conv_kernel(UNetImpl* u, int kind);
+int unet_error(UNetImpl* u);
 int unet_get_params(UNetImpl* u, float* host);
 int unet_set_params(UNetImpl* u, const float* host);
 int unet_prepare(UNetImpl* u, int X, int Y, int Z, int count, char* err, size_t errlen);

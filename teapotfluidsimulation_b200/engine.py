@@ -30,7 +30,7 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_unet_set_loss", "pl_set_unet", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
+    "pl_unet_set_loss", "pl_set_unet", "pl_unet_set_conv_kernel", "pl_unet_error", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
     "pl_ensemble_member", "pl_ensemble_advance", "pl_ensemble_enqueue", "pl_ensemble_destroy",
     "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
     L.pl_unet_destroy.restype = None
     L.pl_unet_set_loss.argtypes = [P, C.c_int32]
     L.pl_set_unet.argtypes = [P, P]
+    L.pl_unet_set_conv_kernel.argtypes = [P, C.c_int32]
+    L.pl_unet_error.argtypes = [P]
     L.pl_ensemble_configs.argtypes = [C.c_uint32, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.Config)]
     L.pl_ensemble_create.argtypes = [C.POINTER(abi.Config), C.c_int32, C.POINTER(P)]
     L.pl_ensemble_size.argtypes = [P]
@@ -515,6 +517,7 @@ class PoissonBatch:
 UNET_LAYERS = [(16, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32), (32, 32), (48, 16), (16, 16),
                (16, 16)]  # (input, output) channels of the 11 convolutions, padded to multiples of 16
 UNET_LOSS_L2, UNET_LOSS_ENERGY = 0, 1
+UNET_CONV_TCGEN05, UNET_CONV_MMA_SYNC = 0, 1
 
 
 class UNet:
@@ -525,6 +528,14 @@ class UNet:
         _check(lib().pl_unet_create(seed, C.byref(h)))
         self._h = h
         self.nparams = int(lib().pl_unet_num_params(h))
+
+    def set_conv_kernel(self, kind: int):
+        """UNET_CONV_TCGEN05 (default) or UNET_CONV_MMA_SYNC (the warp-level tensor-core kernels)."""
+        _check(lib().pl_unet_set_conv_kernel(self._h, kind))
+
+    def error(self) -> int:
+        """1 if a tensor-core convolution gave up a bounded wait (pl_unet_error)."""
+        return int(lib().pl_unet_error(self._h))
 
     def set_loss(self, kind: int):
         """UNET_LOSS_L2 (relative squared error) or UNET_LOSS_ENERGY (relative error in the energy norm)."""

@@ -97,3 +97,30 @@ def test_training_lowers_the_loss(engine):
     for _ in range(60):
         last = net.train_step(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), NX, NY, NZ, N, 1e-3)
     assert last < 0.7 * first, (first, last)
+
+
+@pytest.mark.parametrize("shape", [(16, 12, 8, 2), (32, 16, 12, 3)])
+def test_tcgen05_and_mma_sync_kernels_agree(engine, shape):
+    # the two convolution kernels compute the same BF16 products with FP32 accumulation in different
+    # orders: the network's output agrees to BF16 rounding, the loss and gradient closely
+    X, Y, Z, n = shape
+    rng = np.random.default_rng(1)
+    cell = np.full((n, Z, Y, X), 2, np.uint8)
+    cell[:, 1:-1, 1:-1, 1:-1] = rng.choice(np.array([0, 1, 1], np.uint8), size=(n, Z - 2, Y - 2, X - 2))
+    r = (rng.standard_normal(cell.shape) * (cell == 1)).astype(np.float32)
+    e = (rng.standard_normal(cell.shape) * (cell == 1)).astype(np.float32)
+    dc, dr, de = dev(cell), dev(r), dev(e)
+    out = {}
+    for kind in (engine.engine.UNET_CONV_TCGEN05, engine.engine.UNET_CONV_MMA_SYNC):
+        net = engine.engine.UNet(seed=5)
+        net.set_conv_kernel(kind)
+        dz = torch.zeros_like(dr)
+        net.apply(dc.data_ptr(), dr.data_ptr(), dz.data_ptr(), X, Y, Z, n)
+        torch.cuda.synchronize()
+        loss, g = net.gradient(dc.data_ptr(), dr.data_ptr(), de.data_ptr(), X, Y, Z, n)
+        assert net.error() == 0
+        out[kind] = (dz.cpu().numpy().astype(np.float64), loss, g.astype(np.float64))
+    (z0, l0, g0), (z1, l1, g1) = out.values()
+    assert np.linalg.norm(z0 - z1) <= 1e-2 * np.linalg.norm(z1)
+    assert abs(l0 - l1) <= 1e-3 * abs(l1)
+    assert float(g0 @ g1 / (np.linalg.norm(g0) * np.linalg.norm(g1))) > 0.999
