@@ -324,6 +324,12 @@ int pl_read_particles_f64(pl_sim* sim, double* x, double* y, double* z, double* 
                           double* vz, uint8_t* status);
 /* Simulation3D.origin (solver3d.ts:81): origin layer 0/1/2 per parcel id. */
 int pl_read_origin(const pl_sim* sim, uint8_t* origin);
+/* A recording frame (scripts/record3d.ts capture(), quantised as encodeRecording stores it,
+ * src/view3d/format.ts:60): for every stride-th parcel in id order (k = 0, 1, ... for ids 0, stride,
+ * 2 stride, ...), xyz3[3k + a] = max(0, min(65535, round(position_a / quantum))), positions in the
+ * simulation frame as Float32, rounding halves up as Math.round does. xyz3 holds 3 * ceil(n / stride)
+ * values. The quantisation runs on the device; 6 bytes per kept parcel cross to the host. */
+int pl_read_quantized_positions(pl_sim* sim, int32_t stride, double quantum, uint16_t* xyz3);
 /* readRenderPositions() (src/gpu3d/solver.ts:443-475; kernel src/gpu3d/shaders.ts:786-799):
  * packed xyz of the simulated half then its mirror image, 6*n floats (PL_DOMAIN_FULL: the xyz of
  * the n simulated parcels, 3*n floats), written by a device kernel into a device buffer and copied

@@ -782,6 +782,22 @@ int pl_read_origin(const pl_sim* s, uint8_t* origin) {
   return PL_OK;
 }
 
+int pl_read_quantized_positions(pl_sim* s, int32_t stride, double quantum, uint16_t* xyz3) {
+  if (!s || !xyz3 || stride < 1 || !(quantum > 0))
+    return fail(PL_E_ARG, "pl_read_quantized_positions: bad argument");
+  cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
+  const int n = s->g.n;
+  const int kept = (n + stride - 1) / stride;
+  uint16_t* dev = reinterpret_cast<uint16_t*>(s->P.render);  // scratch: 6 bytes per kept parcel <= 12 n
+  pl::launch_quantize(s->P, n, stride, quantum, dev, s->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(xyz3, dev, size_t(kept) * 6, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return PL_OK;
+}
+
 int pl_read_render_positions(pl_sim* s, float* xyz6n) {
   if (!s || !xyz6n) return fail(PL_E_ARG, "pl_read_render_positions: null argument");
   cudaSetDevice(s->device);

@@ -1037,4 +1037,31 @@ void launch_export_correction(const Geo& g, const DevPtrs& P, float* out, cudaSt
   k_export_correction<<<blocks(g.nf, 256), 256, 0, st>>>(g, P, out);
 }
 
+// ---------------------------------------------------------------- recording frames
+
+// Every stride-th parcel (in id order) quantised as the recording format stores it (format.ts:60):
+// max(0, min(65535, Math.round(f / quantum))) of the FP32 position, the division in FP64 and
+// Math.round's halves toward +infinity; out[3 k + c] for the parcel with id = k * stride.
+__global__ void k_quantize(DevPtrs P, int n, int stride, double quantum, uint16_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = P.pos_home[i];
+  const int id = __float_as_int(p.w);
+  if (id < 0 || id >= n || id % stride) return;
+  const int k = id / stride;
+  const float c[3] = {p.x, p.y, p.z};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double t = double(c[a]) / quantum;
+    double r = floor(t);
+    if (t - r >= 0.5) r += 1.0;
+    r = fmin(fmax(r, 0.0), 65535.0);
+    out[3 * k + a] = uint16_t(r);
+  }
+}
+
+void launch_quantize(const DevPtrs& P, int n, int stride, double quantum, uint16_t* out, cudaStream_t st) {
+  k_quantize<<<(n + 255) / 256, 256, 0, st>>>(P, n, stride, quantum, out);
+}
+
 }  // namespace pl

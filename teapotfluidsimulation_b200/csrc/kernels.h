@@ -47,6 +47,8 @@ void launch_stage_density(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_stage_advect(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
+// recording frames: every stride-th parcel's position quantised to u16 (format.ts:60)
+void launch_quantize(const DevPtrs& P, int n, int stride, double quantum, uint16_t* out, cudaStream_t st);
 struct PoissonImpl;
 // grid-scale solves (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED): the liquid system in the dense box,
 // solved by the Poisson batch's device-driven multigrid / learned PCG inside the substep graph

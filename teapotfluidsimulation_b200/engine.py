@@ -30,7 +30,7 @@ EXPORTED = [
     "pl_stage_times", "pl_plan", "pl_autotune_solver", "pl_pcg_solve_device_noalloc",
     "pl_get_affine", "pl_set_affine", "pl_unet_create", "pl_unet_num_params", "pl_unet_get_params",
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
-    "pl_unet_set_loss", "pl_set_unet", "pl_unet_set_conv_kernel", "pl_unet_error", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
+    "pl_unet_set_loss", "pl_set_unet", "pl_unet_set_conv_kernel", "pl_unet_error", "pl_read_quantized_positions", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
     "pl_ensemble_member", "pl_ensemble_advance", "pl_ensemble_enqueue", "pl_ensemble_destroy",
     "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
     L.pl_unet_set_loss.argtypes = [P, C.c_int32]
     L.pl_set_unet.argtypes = [P, P]
     L.pl_unet_set_conv_kernel.argtypes = [P, C.c_int32]
+    L.pl_read_quantized_positions.argtypes = [P, C.c_int32, C.c_double, C.POINTER(C.c_uint16)]
     L.pl_unet_error.argtypes = [P]
     L.pl_ensemble_configs.argtypes = [C.c_uint32, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.Config)]
     L.pl_ensemble_create.argtypes = [C.POINTER(abi.Config), C.c_int32, C.POINTER(P)]
@@ -324,6 +325,13 @@ class Simulation3D:
         o = np.zeros(self.n, np.uint8)
         _check(lib().pl_read_origin(self._h, _ptr(o, C.c_uint8)))
         return o
+
+    def quantized_positions(self, stride: int = 3, quantum: float = 0.00025) -> np.ndarray:
+        """A recording frame (pl_read_quantized_positions): every stride-th parcel's position as the
+        recording format quantises it, 3 * ceil(n / stride) integers."""
+        out = np.zeros(3 * ((self.n + stride - 1) // stride), np.uint16)
+        _check(lib().pl_read_quantized_positions(self._h, stride, quantum, _ptr(out, C.c_uint16)))
+        return out.astype(np.int64)
 
     def read_render_positions(self) -> np.ndarray:
         """readRenderPositions() (src/gpu3d/solver.ts:443-475): xyz of the half, then the mirror (full

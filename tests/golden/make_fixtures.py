@@ -5,7 +5,8 @@ Reads the reference's committed results (run with the reference mounted at /root
   benchmarks/gpu3d.json      the CPU state after 200 substeps at 5 mm (stepComparison.cpu)
   public/data/pour3d.bin.gz  the 5 mm recording (format: src/view3d/format.ts:4-8): origin tags
                              of every 3rd parcel and 10 fps frames of their positions
-and writes tests/golden/reference_goldens.json and tests/golden/pour3d_early.npz.
+and writes tests/golden/reference_goldens.json, tests/golden/pour3d_early.npz and
+tests/golden/recording_pin.json.
 """
 import gzip
 import json
@@ -39,9 +40,18 @@ def main():
         cur = cur + d
         frames.append(cur.copy())
     f0 = frames[0].astype(np.uint16)
+    # the first bytes of the file exactly (header, origin tags, frame 0, the frame 1 deltas): pins the
+    # recording writer byte for byte; frame 1 itself goes into the npz
+    import hashlib
+
+    pre = 4 + hl + P + 2 * 6 * P
+    pin = {"header_json": raw[4:4 + hl].decode("utf-8"), "prefix_bytes": pre,
+           "prefix_sha256": hashlib.sha256(raw[:pre]).hexdigest()}
+    with open(os.path.join(OUT, "recording_pin.json"), "w") as f:
+        json.dump(pin, f, indent=1)
     deltas = np.stack([frames[k] - frames[0] for k in FRAMES[1:]]).astype(np.int16)
     np.savez_compressed(os.path.join(OUT, "pour3d_early.npz"), origin=origin, frame0=f0, deltas=deltas,
-                        frame_index=np.array(FRAMES))
+                        frame_index=np.array(FRAMES), frame1_delta=(frames[1] - frames[0]).astype(np.int16))
     gold = {
         "source": "marcelpetrick/teapotFluidSimulation benchmarks/run3d.json, benchmarks/gpu3d.json, "
                   "public/data/pour3d.bin.gz",
