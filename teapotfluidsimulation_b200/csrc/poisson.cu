@@ -59,6 +59,15 @@ namespace {
 constexpr int PMAXLEV = 8;
 constexpr int PT = 256;  // cells per tile = threads per CTA
 constexpr int RED_T = 256;
+// Programmatic dependent launch inside the iteration loop: every kernel of the loop body first waits
+// (in every CTA, before any early return) until its predecessor in the stream has completed and its
+// writes are visible, then lets its own successor begin launching; the successor's launch and CTA
+// set-up overlap this kernel's work. Waiting in every CTA keeps the ordering transitive. Launched
+// without the attribute, both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 constexpr int COARSE_SWEEPS = 10;  // (red, black) pairs before and (black, red) pairs after: 40 half-sweeps
 constexpr int MG_NU = 2;           // smoothing sweeps before and after the coarse correction
 constexpr double MG_OMEGA = 1.5;   // over-relaxation of the coarse correction
@@ -348,6 +357,7 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                    const T* w, const T* dg, int cells, T* x, const T* b,
                                                    int color, int first, const Snap* st, const int* nact) {
+  pdl_enter();
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
   if (ti >= *nact) return;
   const int gt = list[ti];
@@ -379,6 +389,7 @@ __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* lis
                                                      const uint8_t* diagf, const T* wf, const T* dgf, int cellsf,
                                                      const T* xf, const T* bf, const uint8_t* codec, T* bc,
                                                      const Snap* st, const int* nact) {
+  pdl_enter();
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
   if (ti >= *nact) return;
   const int gt = listc[ti];
@@ -412,6 +423,7 @@ __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* lis
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* listf, const uint8_t* codef, T* xf,
                                                     const uint8_t* codec, const T* xc, const Snap* st, const int* nact) {
+  pdl_enter();
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
   if (ti >= *nact) return;
   const int gt = listf[ti];
@@ -431,6 +443,7 @@ __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* list
 template <typename T>
 __global__ void __launch_bounds__(1024) k_mg_coarsest(TG G, const uint8_t* code, const T* w, const T* dg,
                                                        int cells, T* x, const T* b, const Snap* st) {
+  pdl_enter();
   __shared__ T sx[512];
   const int s = blockIdx.x;
   if (st[s].done) return;
@@ -614,6 +627,7 @@ __global__ void __launch_bounds__(PT) k_pcg_init(TG G, const int* list, const ui
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint8_t* code, const T* r, const T* z,
                                                const T* rold, double* part, double* part2, const Snap* st, const int* nact) {
+  pdl_enter();
   PCG_TILE_PROLOGUE
   double v = 0, v2 = 0;
   if (live) {
@@ -635,6 +649,7 @@ __global__ void __launch_bounds__(PT) k_pcg_rz(TG G, const int* list, const uint
 template <typename T>
 __global__ void __launch_bounds__(PT) k_select_pre(TG G, const int* list, const uint8_t* code, const float* zn, T* z,
                                                    const Snap* st, const int* nact) {
+  pdl_enter();
   PCG_TILE_PROLOGUE
   if (!live || st[snap].pre) return;
 #pragma unroll
@@ -651,6 +666,7 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                 const T* z, const T* pold, T* pnew, T* ap, double* part,
                                                 const Snap* st, const int* nact) {
+  pdl_enter();
   PCG_TILE_PROLOGUE
   double v = 0;
   if (live) {
@@ -680,6 +696,7 @@ __global__ void __launch_bounds__(PT) k_pcg_pap(TG G, const int* list, const uin
 template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_update(TG G, const int* list, const uint8_t* code, double* x, const T* p,
                                                    T* r, const T* ap, T* rold, double* part, const Snap* st, const int* nact) {
+  pdl_enter();
   PCG_TILE_PROLOGUE
   double v = 0;
   if (live) {
@@ -704,6 +721,7 @@ template <typename T>
 __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                  const float* b, const double* x, T* r, double* part,
                                                  const Snap* st, const int* nact) {
+  pdl_enter();
   PCG_TILE_PROLOGUE
   const bool chk = live && st[snap].check;
   double v = 0;
@@ -727,6 +745,7 @@ __global__ void __launch_bounds__(PT) k_pcg_true(TG G, const int* list, const ui
 // (alpha, breakdown); 3: after the update (max|r|: convergence, check); 4: after a true residual.
 __global__ void __launch_bounds__(RED_T) k_pcg_scalar(int phase, const double* part, const double* part2,
                                                       long long ntile, Snap* st, double tol, int max_iter, int learned) {
+  pdl_enter();
   const int s = blockIdx.x;
   Snap& S = st[s];
   __shared__ double sw[RED_T / 32];
@@ -832,6 +851,7 @@ __global__ void k_snap_result(const Snap* st, double* out) {
 // more than `cap` passes (every snapshot stops at its iteration cap well before; the count is a hard
 // bound on the loop whatever the state holds).
 __global__ void k_loop_next(const Snap* st, int count, int* passes, int cap, cudaGraphConditionalHandle h) {
+  pdl_enter();
   int live = 0;
   for (int s = threadIdx.x; s < count; s += blockDim.x)
     if (!st[s].done) live = 1;
@@ -879,6 +899,23 @@ struct PoissonT : PoissonImpl {
   int* chunk = nullptr;  // per-chunk counts / offsets of the list compaction
   int* pinned = nullptr;
   cudaGraphExec_t iter_graph = nullptr;
+  // A launch of the iteration loop's body: with programmatic stream serialisation (the kernels begin
+  // with pdl_enter) while the body is being recorded, a plain launch otherwise.
+  bool in_loop = false;
+  template <typename... P, typename... A>
+  void lk(void (*k)(P...), unsigned grid, unsigned block, cudaStream_t s, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = in_loop ? at : nullptr;
+    cfg.numAttrs = in_loop ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
+  }
   static unsigned grid2(int nact) { return unsigned(std::max(1, (nact + 1) / 2)); }  // two tiles per CTA
   // Device-driven mode: the active tile counts stay on the device (every launch is sized for all
   // tiles and its CTAs past the count return at once) and the iterations run as a graph while-loop,
@@ -1033,13 +1070,13 @@ struct PoissonT : PoissonImpl {
     char err[128];
     const TG& G = L[0].G;
     unet_apply(net, cell_in, reinterpret_cast<const float*>(r), zn, G.nx, G.ny, G.nz, count, s0, err, sizeof err);
-    k_select_pre<T><<<grid2(lim(0)), PT, 0, s0>>>(G, L[0].list, L[0].code, zn, z, st, nact_d(0));
+    lk(k_select_pre<T>, grid2(lim(0)), PT, s0, G, L[0].list, L[0].code, zn, z, st, nact_d(0));
     // the network's correction, then red-black Gauss-Seidel sweeps from it: the network carries the
     // smooth part of the error, the sweeps the rough part (on a fallen-back snapshot they follow the
     // V-cycle's own post-smoothing)
     for (int q = 0; q < MG_NU; q++)
       for (int color = 0; color < 2; color++)
-        k_mg_smooth<T><<<grid2(lim(0)), PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
+        lk(k_mg_smooth<T>, grid2(lim(0)), PT, s0, G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
                                                      int(count * G.nc), z, r, color, 0, st, nact_d(0));
   }
 
@@ -1056,7 +1093,7 @@ struct PoissonT : PoissonImpl {
     auto B = [&](int l) -> const T* { return l == 0 ? r : L[l].b; };
     auto cells = [&](int l) { return (long long)count * L[l].G.nc; };
     auto smooth = [&](int l, int color, int first) {
-      k_mg_smooth<T><<<grid2(lim(l)), PT, 0, s0>>>(L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
+      lk(k_mg_smooth<T>, grid2(lim(l)), PT, s0, L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
                                                    cells(l), X(l), B(l), color, first, st, nact_d(l));
     };
     const int top = nlev - 1;
@@ -1067,7 +1104,7 @@ struct PoissonT : PoissonImpl {
         smooth(l, 1, 0);
       }
       if (any(l + 1))
-        k_mg_restrict<T><<<grid2(lim(l + 1)), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
+        lk(k_mg_restrict<T>, grid2(lim(l + 1)), PT, s0, L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
                                                           L[l].w, L[l].dg, cells(l), X(l), B(l), L[l + 1].code,
                                                           L[l + 1].b, st, nact_d(l + 1));
     }
@@ -1082,14 +1119,14 @@ struct PoissonT : PoissonImpl {
           smooth(top, 0, 0);
         }
       } else {
-        k_mg_coarsest<T><<<count, 512, 0, s0>>>(L[top].G, L[top].code, L[top].w, L[top].dg, cells(top), X(top), B(top),
+        lk(k_mg_coarsest<T>, count, 512, s0, L[top].G, L[top].code, L[top].w, L[top].dg, cells(top), X(top), B(top),
                                                st);
       }
     }
     for (int l = top - 1; l >= 0; l--) {
       if (!any(l)) continue;
       if (any(l + 1))
-        k_mg_prolong<T><<<grid2(lim(l)), PT, 0, s0>>>(L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
+        lk(k_mg_prolong<T>, grid2(lim(l)), PT, s0, L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
                                                      L[l + 1].code, L[l + 1].x, st, nact_d(l));
       for (int q = 0; q < MG_NU; q++) {
         smooth(l, 1, 0);
@@ -1105,14 +1142,14 @@ struct PoissonT : PoissonImpl {
     const unsigned g0 = grid2(lim(0));
     const int* na = nact_d(0);
     precondition(s0);
-    k_pcg_rz<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, r, z, rold, part, part2, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(1, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_pap<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(2, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_update<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, x, pnew, r, ap, rold, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(3, part, part2, G.ntile, st, tol, max_iter, learned());
-    k_pcg_true<T><<<g0, PT, 0, s0>>>(G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
-    k_pcg_scalar<<<count, RED_T, 0, s0>>>(4, part, part2, G.ntile, st, tol, max_iter, learned());
+    lk(k_pcg_rz<T>, g0, PT, s0, G, L[0].list, L[0].code, r, z, rold, part, part2, st, na);
+    lk(k_pcg_scalar, count, RED_T, s0, 1, part, part2, G.ntile, st, tol, max_iter, learned());
+    lk(k_pcg_pap<T>, g0, PT, s0, G, L[0].list, L[0].code, L[0].diag, z, pold, pnew, ap, part, st, na);
+    lk(k_pcg_scalar, count, RED_T, s0, 2, part, part2, G.ntile, st, tol, max_iter, learned());
+    lk(k_pcg_update<T>, g0, PT, s0, G, L[0].list, L[0].code, x, pnew, r, ap, rold, part, st, na);
+    lk(k_pcg_scalar, count, RED_T, s0, 3, part, part2, G.ntile, st, tol, max_iter, learned());
+    lk(k_pcg_true<T>, g0, PT, s0, G, L[0].list, L[0].code, L[0].diag, b, x, r, part, st, na);
+    lk(k_pcg_scalar, count, RED_T, s0, 4, part, part2, G.ntile, st, tol, max_iter, learned());
   }
 
   // r = b, x = 0, p = p1 = 0 and the per-snapshot state (enqueued on s0, capturable).
@@ -1153,9 +1190,11 @@ struct PoissonT : PoissonImpl {
       cudaGraph_t body = np.conditional.phGraph_out[0];
       e = cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
       if (e == cudaSuccess) {
+        in_loop = true;
         iteration(b, x, tol, max_iter, p, p1, side);
         iteration(b, x, tol, max_iter, p1, p, side);
-        k_loop_next<<<1, 256, 0, side>>>(st, count, passes, max_iter / 2 + 8, h);
+        lk(k_loop_next, 1, 256, side, st, count, passes, max_iter / 2 + 8, h);
+        in_loop = false;
         e = cudaStreamEndCapture(side, &body);
       }
     }
