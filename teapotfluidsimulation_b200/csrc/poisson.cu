@@ -1230,6 +1230,48 @@ struct PoissonT : PoissonImpl {
   // The first snapshot's outcome (iterations, converged, max-norm residual) to device memory.
   void capture_result(double* out3, cudaStream_t s0) override { k_snap_result<<<1, 1, 0, s0>>>(st, out3); }
 
+  struct SolveKey {
+    const void *cell, *b, *x;
+    double tol;
+    int max_iter;
+    int nact[PMAXLEV];
+    bool operator==(const SolveKey& o) const {
+      if (cell != o.cell || b != o.b || x != o.x || tol != o.tol || max_iter != o.max_iter) return false;
+      for (int l = 0; l < PMAXLEV; l++)
+        if (nact[l] != o.nact[l]) return false;
+      return true;
+    }
+  };
+  SolveKey cached{};
+
+  int record_solve(const float* b, double* x, double tol, int max_iter, char* err, size_t errlen) {
+    if (iter_graph) {
+      cudaGraphExecDestroy(iter_graph);
+      iter_graph = nullptr;
+    }
+    int rc = PL_OK;
+    cudaGraph_t gph = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      start(b, x, tol, max_iter, cap);
+      rc = any(0) ? record_loop(b, x, tol, max_iter, cap, err, errlen) : PL_OK;
+      e = cudaStreamEndCapture(cap, &gph);
+      if (rc) e = cudaErrorUnknown;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&iter_graph, gph, 0);
+    if (gph) cudaGraphDestroy(gph);
+    if (cap) cudaStreamDestroy(cap);
+    if (e != cudaSuccess) {
+      if (iter_graph) cudaGraphExecDestroy(iter_graph);
+      iter_graph = nullptr;
+      if (!rc) snprintf(err, errlen, "pl_poisson_solve: solve graph: %s", cudaGetErrorString(e));
+      return rc ? rc : PL_E_CUDA;
+    }
+    return PL_OK;
+  }
+
   int solve(const uint8_t* cell, const float* b, double* x, double tol, int max_iter, cudaStream_t s0, int* iters,
             double* res, int* conv, char* err, size_t errlen) override {
     devmode = false;
@@ -1247,27 +1289,16 @@ struct PoissonT : PoissonImpl {
       rc = unet_prepare(net, L[0].G.nx, L[0].G.ny, L[0].G.nz, count, err, errlen);  // before the capture
       if (rc) return rc;
     }
-    // the whole solve as one graph (start, then the iteration loop), launched once
-    if (iter_graph) {
-      cudaGraphExecDestroy(iter_graph);
-      iter_graph = nullptr;
-    }
-    cudaGraph_t gph = nullptr;
-    cudaStream_t cap = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      start(b, x, tol, max_iter, cap);
-      rc = any(0) ? record_loop(b, x, tol, max_iter, cap, err, errlen) : PL_OK;
-      e = cudaStreamEndCapture(cap, &gph);
-      if (rc) e = cudaErrorUnknown;
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&iter_graph, gph, 0);
-    if (gph) cudaGraphDestroy(gph);
-    if (cap) cudaStreamDestroy(cap);
-    if (e != cudaSuccess) {
-      if (!rc) snprintf(err, errlen, "pl_poisson_solve: solve graph: %s", cudaGetErrorString(e));
-      return rc ? rc : PL_E_CUDA;
+    // the whole solve as one graph (start, then the iteration loop), launched once; the instantiated
+    // graph is kept for the next solve with the same buffers, rule and active-tile counts (the learned
+    // method re-records: its network's workspace may move between solves)
+    SolveKey key{cell, b, x, tol, max_iter, {}};
+    for (int l = 0; l < nlev; l++) key.nact[l] = L[l].nact;
+    cudaError_t e = cudaSuccess;
+    if (!(iter_graph && !learned() && key == cached)) {
+      rc = record_solve(b, x, tol, max_iter, err, errlen);
+      if (rc) return rc;
+      cached = key;
     }
     e = cudaGraphLaunch(iter_graph, s0);
     if (e != cudaSuccess) {

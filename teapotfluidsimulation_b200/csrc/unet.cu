@@ -203,7 +203,7 @@ __host__ __device__ constexpr int tc_cols() {
 constexpr int TC_STAGES = 4;  // (A, B) stages in flight: taps t + 1 .. t + 3 load while tap t multiplies
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 
 template <int NOUT>
@@ -240,21 +240,38 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
   const uint32_t tmem = *tslot;
   const int v = v0 + tid;
   const int kch = cin / 8;  // 16-byte chunks per row
+  // this thread's cell, decomposed once (the taps only add offsets and test the box faces)
+  const int per = B.cells(), XY = B.X * B.Y;
+  const int cl = v < total ? v % per : 0;
+  const int cx = cl % B.X, cy = (cl / B.X) % B.Y, cz = cl / XY;
+  // this thread's share of a tap's weights, at most TC_BMAX 16-byte chunks: shared- and global-memory
+  // offsets computed once
+  constexpr int TC_BMAX = (NOUT * 12 + 127) / 128;  // Cin <= 96
+  uint32_t boff[TC_BMAX];
+  int goff[TC_BMAX];
+  const int nbch = NOUT * kch;
+#pragma unroll
+  for (int q = 0; q < TC_BMAX; q++) {
+    const int e = tid + 128 * q;
+    const int n = e / kch, c = e - n * kch;
+    boff[q] = (c >> 1) * (NOUT * 32) + ((n >> 3) * 2 + (c & 1)) * 128 + (n & 7) * 16;
+    goff[q] = n * cin + 8 * c;
+  }
   // stage s <- tap t: this thread's gathered row (zero-filled outside the box) and its share of the
   // tap's weights, as 16-byte asynchronous copies, one commit group per tap
   auto load_tap = [&](int t, int s) {
     const uint32_t a0 = sbase + s * stage_bytes, b0 = a0 + a_bytes;
-    const int nv = v < total ? tap_cell(B, v, t) : -1;
-    const bf16* src = nv >= 0 ? in + (size_t)nv * cin : in;
-    const uint32_t nbytes = nv >= 0 ? 16u : 0u;
+    const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+    const bool in_box = v < total && (unsigned)(cx + dx) < (unsigned)B.X && (unsigned)(cy + dy) < (unsigned)B.Y &&
+                        (unsigned)(cz + dz) < (unsigned)B.Z;
+    const bf16* src = in_box ? in + (size_t)(v + dx + dy * B.X + dz * XY) * cin : in;
+    const uint32_t nbytes = in_box ? 16u : 0u;
     const uint32_t arow = a0 + (tid >> 3) * 256 + (tid & 7) * 16;
     for (int c = 0; c < kch; c++) cp_async16(arow + (c >> 1) * 4096 + (c & 1) * 128, src + 8 * c, nbytes);
     const bf16* gt = G + (size_t)t * NOUT * cin;
-    for (int e = tid; e < NOUT * kch; e += 128) {
-      const int n = e / kch, c = e - n * kch;
-      cp_async16(b0 + (c >> 1) * (NOUT * 32) + ((n >> 3) * 2 + (c & 1)) * 128 + (n & 7) * 16,
-                 gt + (size_t)n * cin + 8 * c, 16u);
-    }
+#pragma unroll
+    for (int q = 0; q < TC_BMAX; q++)
+      if (tid + 128 * q < nbch) cp_async16(b0 + boff[q], gt + goff[q], 16u);
   };
   for (int p = 0; p < S - 1; p++) {
     load_tap(p, p);

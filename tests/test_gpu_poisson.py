@@ -154,3 +154,29 @@ def test_box_of_a_pour_system(engine, oracle_mod, method):
     assert np.abs(x - q).max() <= 1e-8 * np.abs(q).max()
     if method == 0:
         assert abs(int(it[0]) - oit) <= 1
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_reused_solver_object_repeats_itself(engine, method):
+    # one solver object: snapshots A, then other cells B in the same buffers, then A again, then A
+    # once more (the recorded solve graph is reused when nothing it depends on changed): every solve of
+    # A gives the same iterations and bitwise the same solution
+    E = engine.engine
+    n, count = 32, 3
+    ca, ba = E.poisson_generate(n, 10, count)
+    cb, bb = E.poisson_generate(n, 20, count)
+    dc = torch.from_numpy(ca.copy()).cuda()
+    db = torch.from_numpy(ba.copy()).cuda()
+    dx = torch.zeros((count, n ** 3), dtype=torch.float64, device="cuda")
+    pb = E.PoissonBatch(n, count, method, abi.SOLVE_MIXED)
+    runs = []
+    for cells, rhs in ((ca, ba), (cb, bb), (ca, ba), (ca, ba)):
+        dc.copy_(torch.from_numpy(cells))
+        db.copy_(torch.from_numpy(rhs))
+        it, res, conv = pb.solve(dc.data_ptr(), db.data_ptr(), dx.data_ptr(), 1e-6, 3000)
+        assert conv.all()
+        runs.append((it.copy(), dx.cpu().numpy()))
+    pb.destroy()
+    for k in (2, 3):
+        assert np.array_equal(runs[k][0], runs[0][0]) and np.array_equal(runs[k][1], runs[0][1]), k
+    assert not np.array_equal(runs[1][1], runs[0][1])
