@@ -16,7 +16,9 @@
 //  - k_conv_tc (default): implicit GEMM out[v][n] = bias[n] + sum_t sum_k in[v + off_t][k] G[t][n][k]
 //    on the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 in, FP32 accumulator in tensor
 //    memory), 128 cells x all output channels per CTA, operands staged per tap in shared memory by
-//    asynchronous copies. k_conv computes the same on the warp-level tensor-core path (mma.sync
+//    asynchronous copies through L1 (the dx = -1, 0, +1 taps re-read nearly the same rows);
+//    k_conv_tc_row, for boxes whose x extent is a multiple of 128, instead streams 16 rows per CTA
+//    through a ring of input-row windows. k_conv computes the same on the warp-level path (mma.sync
 //    m16n8k16, one warp per 16 cells), kept for comparison (pl_unet_set_conv_kernel). Both compute the
 //    data gradient with G[t][n][k] = W[26 - t][n][k] (flipped taps).
 //  - k_wgrad: weight gradient dW[t][ci][co] = sum_v in[v + off_t][ci] d[v][co] on the tensor cores:
@@ -195,9 +197,39 @@ __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// Independent accumulators per output tile: tap t accumulates into accumulator t mod TC_NACC, so that
+// consecutive MMAs do not wait on each other's result (a chain of small MMAs into one accumulator is
+// bound by the MMA latency, not its throughput); the epilogue sums them in a fixed order.
 template <int NOUT>
-__host__ __device__ constexpr int tc_cols() {
-  return NOUT <= 32 ? 32 : NOUT <= 64 ? 64 : 128;
+__host__ __device__ constexpr int tc_nacc() {
+  return NOUT <= 32 ? 4 : NOUT <= 64 ? 2 : 1;
+}
+
+// Host copies of tc_cols / tc_nacc for run-time channel counts (shared-memory sizing).
+inline int tc_ncol(int cols) { return cols <= 32 ? 32 : cols <= 64 ? 64 : cols <= 128 ? 128 : cols <= 256 ? 256 : 512; }
+inline int tc_nacc_h(int nout) { return nout <= 32 ? 4 : nout <= 64 ? 2 : 1; }
+
+template <int NOUT>
+__host__ __device__ constexpr int tc_cols() {  // power of two >= 32 that holds NOUT columns
+  return NOUT <= 32 ? 32 : NOUT <= 64 ? 64 : NOUT <= 128 ? 128 : NOUT <= 256 ? 256 : 512;
+}
+
+// Sum of NACC accumulators (NOUT columns apart) for 16 columns of this warp's 32 lanes, in
+// accumulator order.
+template <int NACC, int NOUT>
+__device__ __forceinline__ void tc_ld_sum(uint32_t taddr, float* sum) {
+#pragma unroll
+  for (int a = 0; a < NACC; a++) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr + (uint32_t)(a * NOUT)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; q++) sum[q] = a ? sum[q] + __uint_as_float(r[q]) : __uint_as_float(r[q]);
+  }
 }
 
 constexpr int TC_STAGES = 4;  // (A, B) stages in flight: taps t + 1 .. t + 3 load while tap t multiplies
@@ -212,7 +244,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
                                                  const bf16* __restrict__ mask, bf16* out_bf, float* out_f32,
                                                  int* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  constexpr int NCOL = tc_cols<NOUT>();
+  constexpr int NACC = tc_nacc<NOUT>();
+  constexpr int NCOL = tc_cols<NACC * NOUT>();
   constexpr uint32_t IDESC = tc_idesc<NOUT>();
   constexpr int S = TC_STAGES;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -294,10 +327,10 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
       for (int kc = 0; kc < cin / 16; kc++) {
         const uint64_t ad = tc_desc(a0 + kc * 4096, 128, 256);
         const uint64_t bd = tc_desc(b0 + kc * (NOUT * 32), 128, 256);
-        const uint32_t acc = (t | kc) != 0 ? 1u : 0u;
+        const uint32_t acc = (t >= NACC || kc != 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)((t % NACC) * NOUT)),
             "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
             : "memory");
       }
@@ -329,19 +362,14 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
     for (int c0 = 0; c0 < NOUT; c0 += 16) {
-      uint32_t r[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(lane_base + (uint32_t)c0));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float sum[16];
+      tc_ld_sum<NACC, NOUT>(lane_base + (uint32_t)c0, sum);
       const int vr = v0 + warp * 32 + lane;
       if (vr < total) {
         float f[16];
 #pragma unroll
         for (int q = 0; q < 16; q++) {
-          float x = __uint_as_float(r[q]);
+          float x = sum[q];
           if (bias) x += bias[c0 + q];
           if (relu) x = fmaxf(x, 0.f);
           if (mask && !(__bfloat162float(mask[(size_t)vr * NOUT + c0 + q]) > 0.f)) x = 0.f;
@@ -371,11 +399,206 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
   }
 }
 
+// Row-tile variant for boxes whose x extent is a multiple of 128. A CTA owns a 128-cell segment
+// (x0..x0+127) of TC_RROWS consecutive rows y0..y0+R-1 at fixed z of one box and walks along y: for
+// output row y it needs the input rows y-1, y, y+1 at z-1, z, z+1, each as a window of 130 cells
+// (x0-1..x0+128, zero outside the box). Windows live in a 4-slot ring indexed by y mod 4 (3 windows,
+// one per dz, per slot), so while the MMAs of row y read slots y-1..y+1 the copies of row y+2 fill
+// the fourth: every input row is staged once per CTA instead of 27 times. Tap (dx, dy, dz) is the
+// window (y+dy, dz) read from row dx: a shared-memory descriptor shifted by dx rows (a window holds,
+// per 8-channel group, 130 rows of 16 bytes back to back: 8-row groups 128 B apart, the next group
+// 2080 B on). All 27 taps' weights are staged once per CTA. The accumulator of a row is read back
+// (tcgen05.ld) while the next row's MMAs fill a second accumulator.
+constexpr int TC_WROWS = 130;
+constexpr int TC_RROWS = 16;
+
+template <int NOUT>
+__global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restrict__ in, int cin,
+                                                     const bf16* __restrict__ G, const float* __restrict__ bias,
+                                                     int relu, const bf16* __restrict__ mask, bf16* out_bf,
+                                                     float* out_f32, int* err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  constexpr int NACC = tc_nacc<NOUT>();
+  constexpr int NCOL = tc_cols<2 * NACC * NOUT>();  // two rows' accumulator sets
+  constexpr uint32_t IDESC = tc_idesc<NOUT>();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kch = cin / 8;
+  const int win_bytes = kch * TC_WROWS * 16;  // one window (one input row, one dz)
+  const int slot_bytes = 3 * win_bytes;       // the three dz windows of one input row y
+  const int tap_bytes = NOUT * cin * 2;       // one tap's weights
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t bbase = sbase + 4 * slot_bytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 4 * slot_bytes + 27 * tap_bytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+  // CTA -> (box, z, row block, x segment)
+  const int xseg = B.X / 128, yblk = (B.Y + TC_RROWS - 1) / TC_RROWS;
+  int b = blockIdx.x;
+  const int xs = b % xseg;
+  b /= xseg;
+  const int yb = b % yblk;
+  b /= yblk;
+  const int z = b % B.Z, sb = b / B.Z;
+  const int x0 = xs * 128, y0 = yb * TC_RROWS, y1 = min(B.Y, y0 + TC_RROWS);
+  const size_t box0 = (size_t)sb * B.cells();
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(NCOL)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
+  // input row yy (all three dz) into its ring slot; chunk e = (dz, row, c), c fastest, so consecutive
+  // threads read consecutive 16-byte chunks (a cell's channels, then the next cell's)
+  const int wchunks = TC_WROWS * kch;
+  auto load_row = [&](int yy) {
+    const uint32_t slot = sbase + (yy & 3) * slot_bytes;
+    for (int e = tid; e < 3 * wchunks; e += 128) {
+      const int w = e / wchunks, rem = e - w * wchunks;
+      const int row = rem / kch, c = rem - row * kch;
+      const int zz = z + w - 1, xx = x0 - 1 + row;
+      const bool ok = (unsigned)yy < (unsigned)B.Y && (unsigned)zz < (unsigned)B.Z && (unsigned)xx < (unsigned)B.X;
+      const bf16* src = ok ? in + (box0 + (size_t)(zz * B.Y + yy) * B.X + xx) * cin + 8 * c : in;
+      cp_async16(slot + w * win_bytes + c * (TC_WROWS * 16) + row * 16, src, ok ? 16u : 0u);
+    }
+  };
+  for (int e = tid; e < 27 * NOUT * kch; e += 128) {  // all 27 taps' weights, canonical layout
+    const int t = e / (NOUT * kch), rem = e - t * (NOUT * kch);
+    const int n = rem / kch, c = rem - n * kch;
+    cp_async16(bbase + t * tap_bytes + (c >> 1) * (NOUT * 32) + ((n >> 3) * 2 + (c & 1)) * 128 + (n & 7) * 16,
+               G + (size_t)t * NOUT * cin + (size_t)n * cin + 8 * c, 16u);
+  }
+  load_row(y0 - 1);
+  load_row(y0);
+  load_row(y0 + 1);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  // two sets of NACC accumulators (row parity): the MMAs of row y run while the epilogue of row y - 1
+  // reads the other set
+  auto epilogue = [&](int y, uint32_t acc_col) {
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16) + acc_col;
+    const size_t vr = box0 + (size_t)(z * B.Y + y) * B.X + x0 + warp * 32 + lane;
+#pragma unroll
+    for (int c0 = 0; c0 < NOUT; c0 += 16) {
+      float sum[16];
+      tc_ld_sum<NACC, NOUT>(lane_base + (uint32_t)c0, sum);
+      float f[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        float x = sum[q];
+        if (bias) x += bias[c0 + q];
+        if (relu) x = fmaxf(x, 0.f);
+        if (mask && !(__bfloat162float(mask[vr * NOUT + c0 + q]) > 0.f)) x = 0.f;
+        f[q] = x;
+      }
+      if (out_f32) {
+        float4* o = reinterpret_cast<float4*>(out_f32 + vr * NOUT + c0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) o[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+      }
+      if (out_bf) {
+        __align__(16) bf16 h[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) h[q] = __float2bfloat16(f[q]);
+        uint4* o = reinterpret_cast<uint4*>(out_bf + vr * NOUT + c0);
+        o[0] = *reinterpret_cast<uint4*>(&h[0]);
+        o[1] = *reinterpret_cast<uint4*>(&h[8]);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");  // reads done before that buffer's next MMAs
+  };
+  bool failed = false;
+  int last = -1;  // row whose accumulator still waits for its epilogue
+  for (int y = y0; y < y1; y++) {
+    const int k = y - y0;
+    asm volatile("cp.async.wait_all;" ::: "memory");  // rows y-1..y+1 (and the weights) landed
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();  // also: the epilogue of row y - 2 (the same accumulator) has read it
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t dacc = tmem + (uint32_t)((k & 1) * NACC * NOUT);
+      for (int t = 0; t < 27; t++) {
+        const int dy = (t / 3) % 3, dz = t / 9, dx = t % 3;  // each 0..2 (offset + 1)
+        const uint32_t wa = sbase + ((y - 1 + dy) & 3) * slot_bytes + dz * win_bytes + dx * 16;
+        for (int kc = 0; kc < cin / 16; kc++) {
+          const uint64_t ad = tc_desc(wa + (2 * kc) * (TC_WROWS * 16), TC_WROWS * 16, 128);
+          const uint64_t bd = tc_desc(bbase + t * tap_bytes + kc * (NOUT * 32), 128, 256);
+          const uint32_t acc = (t >= NACC || kc != 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dacc + (uint32_t)((t % NACC) * NOUT)),
+              "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[k & 1]))
+                   : "memory");
+    }
+    if (last >= 0) {
+      // row y - 1: its MMAs done, then its ring slot (y - 2) & 3 is free for row y + 2 and its
+      // accumulator can be read
+      const int kl = last - y0;
+      const bool done = tc_wait(&mbar[kl & 1], uint32_t((kl >> 1) & 1));
+      if (__syncthreads_or(done ? 0 : 1)) {
+        failed = true;
+        break;
+      }
+      if (y + 1 < y1) load_row(y + 2);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(last, (uint32_t)((kl & 1) * NACC * NOUT));
+    } else if (y + 1 < y1) {
+      load_row(y + 2);  // slot (y0 + 2) & 3 has not been used
+    }
+    last = y;
+  }
+  if (!failed && last >= 0) {
+    const int kl = last - y0;
+    const bool done = tc_wait(&mbar[kl & 1], uint32_t((kl >> 1) & 1));
+    if (__syncthreads_or(done ? 0 : 1)) {
+      failed = true;
+    } else {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(last, (uint32_t)((kl & 1) * NACC * NOUT));
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (failed) {
+    if (tid == 0) atomicExch(err, 1);
+    for (int q = 0; q < 2; q++) tc_wait(&mbar[q], 0u), tc_wait(&mbar[q], 1u);  // MMAs in flight (bounded)
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOL) : "memory");
+  }
+}
+
+// Shared memory of k_conv_tc_row: the 4 ring slots (3 windows each), 27 taps' weights, the mbarrier
+// and the TMEM address; with the floor of k_conv_tc so that the resident CTAs fit the SM's
+// tensor-memory columns.
+inline size_t tc_row_smem(int cin, int nout) {
+  const size_t need = size_t(12) * (cin / 8) * TC_WROWS * 16 + size_t(27) * nout * cin * 2 + 64;
+  const int ncol = tc_ncol(2 * tc_nacc_h(nout) * nout);  // two rows' accumulator sets
+  const size_t floor_b = size_t(233472) / size_t(512 / ncol) + 1024;
+  return std::max(need, ncol > 32 ? floor_b : need);
+}
+
+inline unsigned tc_row_blocks(const Box& B) {
+  return unsigned((B.X / 128) * ((B.Y + TC_RROWS - 1) / TC_RROWS) * B.Z * B.count);
+}
+
 // Dynamic shared memory of k_conv_tc: TC_STAGES (A, B) stages, the mbarriers and the TMEM address; at
 // least enough that no more CTAs share an SM than its 512 tensor-memory columns serve.
 inline size_t tc_smem(int cin, int nout) {
   const size_t need = TC_STAGES * (size_t(128) * cin * 2 + size_t(nout) * cin * 2) + 8 * TC_STAGES + 64;
-  const int ncol = nout <= 32 ? 32 : nout <= 64 ? 64 : 128;
+  const int ncol = tc_ncol(tc_nacc_h(nout) * nout);
   const size_t floor_b = size_t(233472) / size_t(512 / ncol) + 1024;
   return std::max(need, ncol > 32 ? floor_b : need);
 }
@@ -842,6 +1065,9 @@ struct UNetImpl {
     cudaFuncSetAttribute(k_conv_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_conv_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_conv_tc<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     // He initialisation from a fixed generator (mulberry32 + Box-Muller); real input channels only
     std::vector<float> h(nparam, 0.f);
     uint32_t a = seed;
@@ -935,6 +1161,18 @@ struct UNetImpl {
   // out = conv_l(in) (forward, G = gf) or the data gradient (G = gb; then nout = cin of the layer).
   void conv(const Box& B, const bf16* in, int cin, const bf16* G, int nout, const float* bias, int relu,
             const bf16* mask, bf16* out_bf, float* out_f32, cudaStream_t st) {
+    if (conv_kernel == PL_UNET_CONV_TCGEN05 && B.X % 128 == 0 && (nout == 16 || nout == 32 || nout == 48) &&
+        tc_row_smem(cin, nout) <= size_t(227 * 1024)) {
+      const unsigned blocks = tc_row_blocks(B);
+      const size_t sm = tc_row_smem(cin, nout);
+      if (nout == 16)
+        k_conv_tc_row<16><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else if (nout == 32)
+        k_conv_tc_row<32><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else
+        k_conv_tc_row<48><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      return;
+    }
     if (conv_kernel == PL_UNET_CONV_TCGEN05) {
       const unsigned blocks = nb(B.total(), 128);
       const size_t sm = tc_smem(cin, nout);

@@ -99,10 +99,11 @@ def test_training_lowers_the_loss(engine):
     assert last < 0.7 * first, (first, last)
 
 
-@pytest.mark.parametrize("shape", [(16, 12, 8, 2), (32, 16, 12, 3)])
+@pytest.mark.parametrize("shape", [(16, 12, 8, 2), (32, 16, 12, 3), (128, 8, 12, 2), (256, 4, 8, 1)])
 def test_tcgen05_and_mma_sync_kernels_agree(engine, shape):
     # the two convolution kernels compute the same BF16 products with FP32 accumulation in different
-    # orders: the network's output agrees to BF16 rounding, the loss and gradient closely
+    # orders: the network's output agrees to BF16 rounding, the loss and gradient closely (x extents
+    # of 128 and 256 take the row-tile tcgen05 kernel at full resolution, the others the gather kernel)
     X, Y, Z, n = shape
     rng = np.random.default_rng(1)
     cell = np.full((n, Z, Y, X), 2, np.uint8)
