@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
                                                  const bf16* __restrict__ mask, bf16* out_bf, float* out_f32,
                                                  int* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  constexpr int NACC = tc_nacc<NOUT>();
+  constexpr int NACC = 1;  // one accumulator: more resident CTAs beat independent chains here
   constexpr int NCOL = tc_cols<NACC * NOUT>();
   constexpr uint32_t IDESC = tc_idesc<NOUT>();
   constexpr int S = TC_STAGES;
@@ -598,7 +598,7 @@ inline unsigned tc_row_blocks(const Box& B) {
 // least enough that no more CTAs share an SM than its 512 tensor-memory columns serve.
 inline size_t tc_smem(int cin, int nout) {
   const size_t need = TC_STAGES * (size_t(128) * cin * 2 + size_t(nout) * cin * 2) + 8 * TC_STAGES + 64;
-  const int ncol = tc_ncol(tc_nacc_h(nout) * nout);
+  const int ncol = tc_ncol(nout);
   const size_t floor_b = size_t(233472) / size_t(512 / ncol) + 1024;
   return std::max(need, ncol > 32 ? floor_b : need);
 }
