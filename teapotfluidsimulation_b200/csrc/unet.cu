@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
                                                  const bf16* __restrict__ mask, bf16* out_bf, float* out_f32,
                                                  int* err) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  constexpr int NACC = 1;  // one accumulator: more resident CTAs beat independent chains here
+  constexpr int NACC = 1;  // one accumulator and one issuing thread: more resident CTAs
   constexpr int NCOL = tc_cols<NACC * NOUT>();
   constexpr uint32_t IDESC = tc_idesc<NOUT>();
   constexpr int S = TC_STAGES;
@@ -327,10 +327,10 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
       for (int kc = 0; kc < cin / 16; kc++) {
         const uint64_t ad = tc_desc(a0 + kc * 4096, 128, 256);
         const uint64_t bd = tc_desc(b0 + kc * (NOUT * 32), 128, 256);
-        const uint32_t acc = (t >= NACC || kc != 0) ? 1u : 0u;
+        const uint32_t acc = (t | kc) != 0 ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)((t % NACC) * NOUT)),
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
             "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
             : "memory");
       }
@@ -407,13 +407,15 @@ __global__ void __launch_bounds__(128) k_conv_tc(Box B, const bf16* __restrict__
 // the fourth: every input row is staged once per CTA instead of 27 times. Tap (dx, dy, dz) is the
 // window (y+dy, dz) read from row dx: a shared-memory descriptor shifted by dx rows (a window holds,
 // per 8-channel group, 130 rows of 16 bytes back to back: 8-row groups 128 B apart, the next group
-// 2080 B on). All 27 taps' weights are staged once per CTA. The accumulator of a row is read back
-// (tcgen05.ld) while the next row's MMAs fill a second accumulator.
+// 2080 B on). All 27 taps' weights are staged once per CTA. The taps go round-robin into NACC
+// independent accumulators, each issued by its own warp (one tcgen05.mma issue costs a few hundred
+// cycles, so a single issuing thread was the row's critical path); the accumulators of a row are read
+// back (tcgen05.ld) while the next row's MMAs fill a second set.
 constexpr int TC_WROWS = 130;
 constexpr int TC_RROWS = 16;
 
-template <int NOUT>
-__global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restrict__ in, int cin,
+template <int CIN, int NOUT>
+__global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restrict__ in, int,
                                                      const bf16* __restrict__ G, const float* __restrict__ bias,
                                                      int relu, const bf16* __restrict__ mask, bf16* out_bf,
                                                      float* out_f32, int* err) {
@@ -422,10 +424,10 @@ __global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restri
   constexpr int NCOL = tc_cols<2 * NACC * NOUT>();  // two rows' accumulator sets
   constexpr uint32_t IDESC = tc_idesc<NOUT>();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int kch = cin / 8;
+  constexpr int cin = CIN, kch = CIN / 8;
   const int win_bytes = kch * TC_WROWS * 16;  // one window (one input row, one dz)
   const int slot_bytes = 3 * win_bytes;       // the three dz windows of one input row y
-  const int tap_bytes = NOUT * cin * 2;       // one tap's weights
+  constexpr int tap_bytes = NOUT * CIN * 2;  // one tap's weights
   const uint32_t sbase = smem_u32(smem);
   const uint32_t bbase = sbase + 4 * slot_bytes;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 4 * slot_bytes + 27 * tap_bytes);
@@ -441,8 +443,8 @@ __global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restri
   const int x0 = xs * 128, y0 = yb * TC_RROWS, y1 = min(B.Y, y0 + TC_RROWS);
   const size_t box0 = (size_t)sb * B.cells();
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[0])), "r"(NACC) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[1])), "r"(NACC) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -519,19 +521,20 @@ __global__ void __launch_bounds__(128) k_conv_tc_row(Box B, const bf16* __restri
     asm volatile("cp.async.wait_all;" ::: "memory");  // rows y-1..y+1 (and the weights) landed
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();  // also: the epilogue of row y - 2 (the same accumulator) has read it
-    if (tid == 0) {
+    if (lane == 0 && warp < NACC) {  // warp a issues the taps of accumulator a (t = a mod NACC)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t dacc = tmem + (uint32_t)((k & 1) * NACC * NOUT);
-      for (int t = 0; t < 27; t++) {
+      const uint32_t dacc = tmem + (uint32_t)((k & 1) * NACC * NOUT + warp * NOUT);
+      for (int t = warp; t < 27; t += NACC) {
         const int dy = (t / 3) % 3, dz = t / 9, dx = t % 3;  // each 0..2 (offset + 1)
         const uint32_t wa = sbase + ((y - 1 + dy) & 3) * slot_bytes + dz * win_bytes + dx * 16;
-        for (int kc = 0; kc < cin / 16; kc++) {
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; kc++) {
           const uint64_t ad = tc_desc(wa + (2 * kc) * (TC_WROWS * 16), TC_WROWS * 16, 128);
           const uint64_t bd = tc_desc(bbase + t * tap_bytes + kc * (NOUT * 32), 128, 256);
           const uint32_t acc = (t >= NACC || kc != 0) ? 1u : 0u;
           asm volatile(
               "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dacc + (uint32_t)((t % NACC) * NOUT)),
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dacc),
               "l"(ad), "l"(bd), "r"(IDESC), "r"(acc)
               : "memory");
         }
@@ -1065,9 +1068,9 @@ struct UNetImpl {
     cudaFuncSetAttribute(k_conv_tc<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_conv_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(k_conv_tc<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_conv_tc_row<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_conv_tc_row<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(k_conv_tc_row<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<16, 48>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(k_conv_tc_row<48, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     // He initialisation from a fixed generator (mulberry32 + Box-Muller); real input channels only
     std::vector<float> h(nparam, 0.f);
     uint32_t a = seed;
@@ -1161,16 +1164,17 @@ struct UNetImpl {
   // out = conv_l(in) (forward, G = gf) or the data gradient (G = gb; then nout = cin of the layer).
   void conv(const Box& B, const bf16* in, int cin, const bf16* G, int nout, const float* bias, int relu,
             const bf16* mask, bf16* out_bf, float* out_f32, cudaStream_t st) {
-    if (conv_kernel == PL_UNET_CONV_TCGEN05 && B.X % 128 == 0 && (nout == 16 || nout == 32 || nout == 48) &&
-        tc_row_smem(cin, nout) <= size_t(227 * 1024)) {
+    if (conv_kernel == PL_UNET_CONV_TCGEN05 && B.X % 128 == 0 &&
+        ((cin == 16 && (nout == 16 || nout == 48)) || (cin == 48 && nout == 16))) {
+      // the full-resolution convolutions (and their data gradients) of boxes 128 or 256 wide
       const unsigned blocks = tc_row_blocks(B);
       const size_t sm = tc_row_smem(cin, nout);
-      if (nout == 16)
-        k_conv_tc_row<16><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
-      else if (nout == 32)
-        k_conv_tc_row<32><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      if (cin == 16 && nout == 16)
+        k_conv_tc_row<16, 16><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+      else if (cin == 16)
+        k_conv_tc_row<16, 48><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
       else
-        k_conv_tc_row<48><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
+        k_conv_tc_row<48, 16><<<blocks, 128, sm, st>>>(B, in, cin, G, bias, relu, mask, out_bf, out_f32, dev_err);
       return;
     }
     if (conv_kernel == PL_UNET_CONV_TCGEN05) {
