@@ -132,7 +132,9 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+
+        self.path = os.path.join(tempfile.gettempdir(), f"pourlab_clocks_{os.getpid()}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
