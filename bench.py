@@ -446,6 +446,8 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
     for c in mine:
         c.preconditioner = abi.PRECOND_CHEB
         c.solve_precision = abi.SOLVE_MIXED
+        # 4-CTA clusters: a 5 mm pour solves as fast as on 16, and 4x as many pours' solves fit at once
+        c.solve_cluster, c.solve_threads = 4, 512
         c.device = torch.cuda.current_device()
     t0 = time.perf_counter()
     ens = E.Ensemble(mine)
@@ -476,7 +478,7 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
     ens.destroy()
     total_sim = allsum(sim_s, world)
     return {"workload": f"{args.ensemble_count} seeded gentle pours at {args.ensemble_mm} mm (half pot), "
-                        f"{args.ensemble_steps} substeps each from t = 0.6 s, Chebyshev cluster solves",
+                        f"{args.ensemble_steps} substeps each from t = 0.6 s, Chebyshev solves on 4-CTA clusters",
             "pours": args.ensemble_count, "pours_per_gpu": len(mine), "parcels_per_gpu": parcels,
             "cells_min": min(grids), "cells_max": max(grids), "create_s": create_s,
             "sim_s_per_wall_s": total_sim / wall, "pour_substeps_per_s": allsum(len(mine), world) * args.ensemble_steps / wall,
