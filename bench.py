@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cell-mm", type=float, default=4.0)
     ap.add_argument("--precond", default="cheb", choices=["mic0", "mg", "cheb"])
+    ap.add_argument("--solve-shape", default="16x512",
+                    help="cluster CTAs x threads of the cluster solves, or 'auto' (pl_autotune_solver, untimed)")
     ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"],
                     help="solver vectors: mixed = FP32 stencils/Chebyshev with FP64 inner products and FP64 "
                          "true-residual refinement; f64 = all FP64")
@@ -78,6 +80,14 @@ def make_cfg(args):
     cfg = abi.gentle_pour(args.cell_mm, 20.0)
     cfg.preconditioner = {"mic0": abi.PRECOND_MIC0, "mg": abi.PRECOND_MG, "cheb": abi.PRECOND_CHEB}[args.precond]
     cfg.solve_precision = abi.SOLVE_MIXED if args.precision == "mixed" else abi.SOLVE_F64
+    if args.solve_shape != "auto":
+        cfg.solve_cluster, cfg.solve_threads = (int(v) for v in args.solve_shape.split("x"))
+    else:
+        if not hasattr(make_cfg, "tuned"):
+            from teapotfluidsimulation_b200 import engine as E
+
+            make_cfg.tuned = E.autotune_solver(cfg, 8)[:2]
+        cfg.solve_cluster, cfg.solve_threads = make_cfg.tuned
     return cfg
 
 
@@ -630,6 +640,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": ("f32 solve vectors, f64 inner products/refinement" if args.precision == "mixed" else "f64 solve")
                  + " / f32 parcels and faces, f64 transfer weights", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "preconditioner": args.precond,
+                   "solve_shape": f"{cfg.solve_cluster}x{cfg.solve_threads}",
                    "solve_precision": args.precision,
                    "start_s": args.start, "simulated_s": sim_s, "l2": "256 MiB buffer written between substeps",
                    "parallelism": f"replicas x{world}"},

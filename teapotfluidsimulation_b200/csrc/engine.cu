@@ -473,7 +473,7 @@ int pl_autotune_solver(const pl_config* cfg, int32_t substeps, int32_t* best_clu
   if (!cfg || substeps < 1 || !best_cluster || !best_threads) return fail(PL_E_ARG, "pl_autotune_solver: bad argument");
   pl_config c = *cfg;
   c.preconditioner = PL_PRECOND_CHEB;
-  const int clusters[] = {16, 12, 8};
+  const int clusters[] = {16, 12, 8, 4};
   const int threads[] = {512, 1024, 256};
   float best = INFINITY;
   int bc = 0, bt = 0;
