@@ -257,7 +257,7 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
 
     n, count = args.poisson_n, args.poisson_count
     t0 = time.perf_counter()
-    cell, b = E.poisson_generate(n, rank * count, count)
+    cell, b = E.poisson_generate(n, poisson_first_snapshot(rank, count), count)
     gen_s = time.perf_counter() - t0
     m_each = ((cell & 3) == abi.FLUID).sum(axis=1)  # unknowns per snapshot (border cells are SOLID)
     dc = torch.from_numpy(cell).cuda()
@@ -439,6 +439,17 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
     return out
 
 
+def shard_pours(items: list, rank: int, world: int) -> list:
+    """The pours of an ensemble this rank runs: round-robin over the ranks (no collective on the data
+    path; every pour on exactly one rank)."""
+    return items[rank::world]
+
+
+def poisson_first_snapshot(rank: int, count: int) -> int:
+    """First snapshot index (seed offset) of this rank's share of the Poisson batch."""
+    return rank * count
+
+
 def run_ensemble(args, world: int, rank: int) -> dict | None:
     """A seeded ensemble of pours (fill U[0.6, 1.0] L, peak tilt U[60, 110] deg, tilt-in ramp U[4, 12] s;
     uneven grids), sharded round-robin over the ranks, each pour on its own stream with the substeps of all
@@ -452,7 +463,7 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
     from teapotfluidsimulation_b200 import engine as E
 
     cfgs = E.ensemble_configs(2026, args.ensemble_count, args.ensemble_mm, 20.0)
-    mine = cfgs[rank::world]
+    mine = shard_pours(cfgs, rank, world)
     for c in mine:
         c.preconditioner = abi.PRECOND_CHEB
         c.solve_precision = abi.SOLVE_MIXED
