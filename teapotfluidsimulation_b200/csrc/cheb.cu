@@ -552,7 +552,9 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     *zr = pr;
     *zw = pw;
   };
-  for (int job = 0; job < a.jobs; job++) {
+  const int cid = int(blockIdx.x) / ns;  // cluster of the launch (two when the jobs run in parallel)
+  const int job0 = a.parallel ? cid : 0, job1 = a.parallel ? cid + 1 : a.jobs;
+  for (int job = job0; job < job1; job++) {
   // job 0: the launch's first system (pressure, or the one system of a single-job launch); job 1:
   // the density correction of the same substep (same liquid cells, so the same exchange tables)
   const bool corr = job == 1 || a.is_correction;
@@ -562,7 +564,7 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   const int jmax = job == 0 ? a.max_iter : a.max_iter2;
   if (job == 1) {
     if (me == 0 && tid == 0) {  // interior mean of the density ratios (solver3d.ts:670)
-      sc->t_solve[1] = globaltimer_ns();
+      if (!a.parallel) sc->t_solve[1] = globaltimer_ns();
       double s = 0;
       int n = 0;
       for (int b = 0; b < DENSITY_BLOCKS; b++) {
@@ -699,9 +701,12 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   }  // jobs
   if (!ok) atomicOr(&sc->errors, ERR_SOLVER_TIMEOUT);  // (exchange waits run in warp 0)
   if (me == 0 && tid == 0) {
-    const unsigned long long t = globaltimer_ns();
-    sc->t_solve[2] = t;
-    if (a.jobs < 2 || !sc->corr_any) sc->t_solve[1] = t;
+    if (cid == 0) {
+      const unsigned long long t = globaltimer_ns();
+      sc->t_solve[2] = t;
+      // one system, or two overlapping ones: the launch's time stays with the solve stage
+      if (a.jobs < 2 || a.parallel || !sc->corr_any) sc->t_solve[1] = t;
+    }
     sc->mg_status = 1;
   }
   cl.sync();  // no rank leaves while another may still address its shared memory
@@ -722,7 +727,7 @@ void configure_one() {
 template <int K>
 void launch_k(const Geo& g, const DevPtrs& P, const SolverWs& W, const ChebArgs& a, cudaStream_t st) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(a.cluster);
+  cfg.gridDim = dim3(a.cluster * (a.parallel ? 2 : 1));
   cfg.blockDim = dim3(std::min(a.threads, CHEB_MAX_THREADS / K));
   cfg.dynamicSmemBytes = a.smem_bytes;
   cfg.stream = st;

@@ -34,6 +34,9 @@ struct ChebArgs {
   double* q2;
   double tol2;
   int max_iter2;
+  // jobs = 2 on two clusters of one launch at once (cluster j solves system j) instead of one after
+  // the other: the two systems are independent, so the launch takes the longer of the two
+  int parallel;
 };
 
 void cheb_configure();

@@ -482,6 +482,7 @@ void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
     c.q2 = P.qc;
     c.tol2 = 1e-4;  // solver3d.ts:673
     c.max_iter2 = 80;
+    c.parallel = 1;
     launch_cheb_solve(g, P, W, c, st);
   }
   SolveArgs a{W.bp, P.q, g.tol, g.max_iter, 0, 1, (mg || cheb) ? 1 : 0};
