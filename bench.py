@@ -358,7 +358,8 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
     """The full-domain APIC pour (both halves of the pot; at 2.5 mm 126 x 126 x 64 cells and 752,630
     parcels) on the grid-scale pressure solves: multigrid PCG, then learned flexible CG (network trained
     here on residual/correction pairs of the same pour, multigrid fall-back) from the same state. Both end
-    every solve on the reference's max-norm 1e-6 rule; device time from the substep graph's stage events."""
+    every solve on the reference's max-norm 1e-6 rule; device time from the substep graph's stage events
+    (the correction solve runs beside the pressure solve, so both are in the "pressure" stage)."""
     if args.full_mm <= 0:
         return None
     import torch

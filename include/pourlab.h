@@ -64,7 +64,8 @@ enum pl_phase {
  * BOX_MG and LEARNED are the grid-scale solves, for any system size: the liquid system is embedded
  * in a dense power-of-two box around the grid and solved there by multigrid PCG (the Poisson
  * batch's Galerkin hierarchy) or by flexible CG with the network of pl_set_unet and that
- * multigrid as the fall-back, the whole solve a while-loop node of the substep's CUDA graph. */
+ * multigrid as the fall-back, the whole solve a while-loop node of the substep's CUDA graph; the
+ * density-correction system runs beside it on a second branch of the graph (multigrid). */
 enum pl_preconditioner {
   PL_PRECOND_MIC0 = 0,
   PL_PRECOND_MG = 1,

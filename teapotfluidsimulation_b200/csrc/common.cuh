@@ -292,6 +292,9 @@ struct DevPtrs {
   float* box_b;
   double* box_x;
   double* box_out;
+  float* box_b2;  // the density-correction solve's rhs, solution and outcome (it runs beside the pressure)
+  double* box_x2;
+  double* box_out2;
   // render
   float* render;
   SimScalars* sc;

@@ -67,6 +67,9 @@ struct pl_sim {
   int pending = 0;  // substeps queued by pl_enqueue_substeps since the last pull
   cudaEvent_t ev[PL_STAGES + 1] = {};
   pl::PoissonImpl* box = nullptr;  // grid-scale solver (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED)
+  pl::PoissonImpl* box2 = nullptr; // ... and the density correction's (multigrid), run beside it
+  cudaStream_t st2 = nullptr;      // the second stream of the substep capture
+  cudaEvent_t fork = nullptr, join = nullptr;
   pl::UNetImpl* net = nullptr;     // its network (PL_PRECOND_LEARNED), owned by the caller
 };
 
@@ -117,17 +120,14 @@ int record_substep(pl_sim* s) {
   launch_stage_density(g, P, st);
   mark(3);
   char err[256] = "";
-  if (g.box_solve) {
-    if (launch_box_pressure(g, P, s->box, st, err, sizeof err)) return fail(PL_E_CUDA, "%s", err);
+  if (g.box_solve) {  // both solves side by side in the pressure stage
+    if (launch_box_solves(g, P, s->box, s->box2, st, s->st2, s->fork, s->join, err, sizeof err))
+      return fail(PL_E_CUDA, "%s", err);
   } else {
     launch_pressure_solve(g, P, st);
   }
   mark(4);
-  if (g.box_solve) {
-    if (launch_box_correction(g, P, s->box, st, err, sizeof err)) return fail(PL_E_CUDA, "%s", err);
-  } else {
-    launch_correction_solve(g, P, st);
-  }
+  if (!g.box_solve) launch_correction_solve(g, P, st);
   mark(5);
   launch_stage_extrap(g, P, st);
   mark(6);
@@ -307,6 +307,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       g.apic ? N * 48 : 16, g.apic ? N * 48 : 16,      // APIC affine vectors (home, sorted)
       g.box_solve ? NB : 16, g.box_solve ? NB * 4 : 16,  // grid-scale solves: box cells, rhs
       g.box_solve ? NB * 8 : 16, 32,                     // box solution, outcome
+      g.box_solve ? NB * 4 : 16, g.box_solve ? NB * 8 : 16, 32,  // the correction's rhs, solution, outcome
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -369,13 +370,22 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.box_b = (float*)take();
   P.box_x = (double*)take();
   P.box_out = (double*)take();
+  P.box_b2 = (float*)take();
+  P.box_x2 = (double*)take();
+  P.box_out2 = (double*)take();
   if (g.box_solve) {
     int brc = 0;
     char berr[256] = "";
     s->box = pl::poisson_create(g.bx, g.by, g.bz, 1,
                                 cfg->preconditioner == PL_PRECOND_LEARNED ? PL_POISSON_LEARNED : PL_POISSON_MG,
                                 g.precision, berr, sizeof berr, &brc);
-    if (!s->box) {
+    if (s->box)  // the correction's own solver: it runs at the same time as the pressure's
+      s->box2 = pl::poisson_create(g.bx, g.by, g.bz, 1, PL_POISSON_MG, g.precision, berr, sizeof berr, &brc);
+    cudaError_t ce = cudaSuccess;
+    if (s->box2) ce = cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking);
+    if (s->box2 && ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
+    if (s->box2 && ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming);
+    if (!s->box || !s->box2 || ce != cudaSuccess) {
       pl_destroy(s);
       return fail(brc ? brc : PL_E_CUDA, "pl_create: grid-scale solver: %s", berr);
     }
@@ -442,6 +452,10 @@ void pl_destroy(pl_sim* s) {
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->exec) cudaGraphExecDestroy(s->exec);
   if (s->box) pl::poisson_destroy(s->box);
+  if (s->box2) pl::poisson_destroy(s->box2);
+  if (s->fork) cudaEventDestroy(s->fork);
+  if (s->join) cudaEventDestroy(s->join);
+  if (s->st2) cudaStreamDestroy(s->st2);
   if (s->mem) cudaFree(s->mem);
   for (int i = 0; i <= PL_STAGES; i++)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);

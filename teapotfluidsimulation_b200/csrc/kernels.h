@@ -52,8 +52,8 @@ void launch_quantize(const DevPtrs& P, int n, int stride, double quantum, uint16
 struct PoissonImpl;
 // grid-scale solves (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED): the liquid system in the dense box,
 // solved by the Poisson batch's device-driven multigrid / learned PCG inside the substep graph
-int launch_box_pressure(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen);
-int launch_box_correction(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen);
+int launch_box_solves(const Geo& g, const DevPtrs& P, PoissonImpl* box, PoissonImpl* box2, cudaStream_t st,
+                      cudaStream_t st2, cudaEvent_t fork, cudaEvent_t join, char* err, size_t errlen);
 void launch_render(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_export_correction(const Geo& g, const DevPtrs& P, float* out, cudaStream_t st);
 

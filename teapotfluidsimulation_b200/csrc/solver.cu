@@ -508,7 +508,7 @@ void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st) {
 // AIR / SOLID elsewhere, SOLID outside the grid (so the box operator is the liquid list's operator:
 // diagonal = non-SOLID neighbours, -1 between liquid neighbours); b = rhs on the liquid cells (0 on an
 // inactive substep, which the solve then finishes at once).
-__global__ void k_box_embed(Geo g, DevPtrs P, const double* rhs, int with_cells) {
+__global__ void k_box_embed(Geo g, DevPtrs P, const double* rhs, int with_cells, float* bout) {
   const long long nb = (long long)g.bx * g.by * g.bz;
   const bool act = P.sc->active != 0;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nb; v += (long long)gridDim.x * blockDim.x) {
@@ -526,13 +526,13 @@ __global__ void k_box_embed(Geo g, DevPtrs P, const double* rhs, int with_cells)
       }
     }
     if (with_cells) P.box_cell[v] = t;
-    P.box_b[v] = b;
+    bout[v] = b;
   }
 }
 
 // The box solution back on the liquid list, and the solve's outcome into the scalar block (the
 // pressure solve counts a failure when it did not converge, solver3d.ts:540).
-__global__ void k_box_finish(Geo g, DevPtrs P, double* q, int correction) {
+__global__ void k_box_finish(Geo g, DevPtrs P, const double* xbox, const double* out, double* q, int correction) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
   const int m = sc->m;
@@ -540,18 +540,18 @@ __global__ void k_box_finish(Geo g, DevPtrs P, double* q, int correction) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
     const int c = P.list[t];
     const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / nxy;
-    q[t] = P.box_x[i + (long long)g.bx * (j + (long long)g.by * k)];
+    q[t] = xbox[i + (long long)g.bx * (j + (long long)g.by * k)];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const int it = int(P.box_out[0]);
-    const double res = P.box_out[2];
+    const int it = int(out[0]);
+    const double res = out[2];
     if (correction) {
       sc->corr_iters = it;
       sc->corr_residual = res;
     } else {
       sc->last_iters = it;
       sc->last_residual = res;
-      if (P.box_out[1] == 0) sc->failures++;
+      if (out[1] == 0) sc->failures++;
     }
   }
 }
@@ -561,25 +561,35 @@ static unsigned box_blocks(const Geo& g) {
   return unsigned(std::min<long long>((nb + 255) / 256, 148 * 16));
 }
 
-int launch_box_pressure(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen) {
+// Both grid-scale solves of a substep. They are independent (the correction's rhs needs only the
+// parcels and the cell types), so after the box's cell types are written the correction forks onto
+// a second stream of the capture with its own solver and buffers (multigrid, tolerance 1e-4,
+// solver3d.ts:673) and joins before the stream goes on: the graph runs the two solves side by side.
+int launch_box_solves(const Geo& g, const DevPtrs& P, PoissonImpl* box, PoissonImpl* box2, cudaStream_t st,
+                      cudaStream_t st2, cudaEvent_t fork, cudaEvent_t join, char* err, size_t errlen) {
   SolverWs W = ws_of(P, g.nc);
   k_solve_setup<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, W, 1, 0);
-  k_box_embed<<<box_blocks(g), 256, 0, st>>>(g, P, W.bp, 1);
-  int rc = poisson_capture_setup(box, P.box_cell, st, err, errlen);
+  k_box_embed<<<box_blocks(g), 256, 0, st>>>(g, P, W.bp, 1, P.box_b);
+  cudaEventRecord(fork, st);
+  cudaStreamWaitEvent(st2, fork, 0);
+  // correction (second stream)
+  k_box_embed<<<box_blocks(g), 256, 0, st2>>>(g, P, P.rhs, 0, P.box_b2);
+  int rc = poisson_capture_setup(box2, P.box_cell, st2, err, errlen);
+  if (!rc) rc = poisson_capture_solve(box2, P.box_b2, P.box_x2, 1e-4, 80, st2, err, errlen);
+  if (!rc) {
+    poisson_capture_result(box2, P.box_out2, st2);
+    k_box_finish<<<DENSITY_BLOCKS, 256, 0, st2>>>(g, P, P.box_x2, P.box_out2, P.qc, 1);
+  }
+  cudaEventRecord(join, st2);
+  // pressure (this stream)
+  if (!rc) rc = poisson_capture_setup(box, P.box_cell, st, err, errlen);
   if (!rc) rc = poisson_capture_solve(box, P.box_b, P.box_x, g.tol, g.max_iter, st, err, errlen);
-  if (rc) return rc;
-  poisson_capture_result(box, P.box_out, st);
-  k_box_finish<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, P.q, 0);
-  return PL_OK;
-}
-
-int launch_box_correction(const Geo& g, const DevPtrs& P, PoissonImpl* box, cudaStream_t st, char* err, size_t errlen) {
-  k_box_embed<<<box_blocks(g), 256, 0, st>>>(g, P, P.rhs, 0);
-  int rc = poisson_capture_solve(box, P.box_b, P.box_x, 1e-4, 80, st, err, errlen);  // solver3d.ts:673
-  if (rc) return rc;
-  poisson_capture_result(box, P.box_out, st);
-  k_box_finish<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, P.qc, 1);
-  return PL_OK;
+  if (!rc) {
+    poisson_capture_result(box, P.box_out, st);
+    k_box_finish<<<DENSITY_BLOCKS, 256, 0, st>>>(g, P, P.box_x, P.box_out, P.q, 0);
+  }
+  cudaStreamWaitEvent(st, join, 0);
+  return rc;
 }
 
 // ---------------------------------------------------------------- standalone solve
