@@ -69,7 +69,8 @@ struct pl_sim {
   pl::PoissonImpl* box = nullptr;  // grid-scale solver (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED)
   pl::PoissonImpl* box2 = nullptr; // ... and the density correction's (multigrid), run beside it
   cudaStream_t st2 = nullptr;      // the second stream of the substep capture
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;    // the grid-scale correction solve's branch
+  cudaEvent_t fork0 = nullptr, join0 = nullptr;  // the density stage's branch
   pl::UNetImpl* net = nullptr;     // its network (PL_PRECOND_LEARNED), owned by the caller
 };
 
@@ -115,9 +116,16 @@ int record_substep(pl_sim* s) {
   mark(0);
   launch_stage_bin(g, P, st);
   mark(1);
-  launch_stage_p2g(g, P, st);
+  // P2G: the cells' node partials, then the faces here and the density stage on the second stream
+  // (both only read the partials); the density stage's event marks the wait for it
+  launch_p2g_cells(g, P, st);
+  cudaEventRecord(s->fork0, st);
+  cudaStreamWaitEvent(s->st2, s->fork0, 0);
+  launch_stage_density(g, P, s->st2);
+  cudaEventRecord(s->join0, s->st2);
+  launch_p2g_faces(g, P, st);
   mark(2);
-  launch_stage_density(g, P, st);
+  cudaStreamWaitEvent(st, s->join0, 0);
   mark(3);
   char err[256] = "";
   if (g.box_solve) {  // both solves side by side in the pressure stage
@@ -279,6 +287,9 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
     e = cudaGetDevice(&s->device);
   if (cfg->device >= 0) s->device = cfg->device;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork0, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->join0, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->pinned, sizeof(SimScalars), cudaHostAllocDefault);
   for (int i = 0; i <= PL_STAGES && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
   if (e != cudaSuccess) {
@@ -382,8 +393,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
     if (s->box)  // the correction's own solver: it runs at the same time as the pressure's
       s->box2 = pl::poisson_create(g.bx, g.by, g.bz, 1, PL_POISSON_MG, g.precision, berr, sizeof berr, &brc);
     cudaError_t ce = cudaSuccess;
-    if (s->box2) ce = cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking);
-    if (s->box2 && ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
+    if (s->box2) ce = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming);
     if (s->box2 && ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming);
     if (!s->box || !s->box2 || ce != cudaSuccess) {
       pl_destroy(s);
@@ -455,6 +465,8 @@ void pl_destroy(pl_sim* s) {
   if (s->box2) pl::poisson_destroy(s->box2);
   if (s->fork) cudaEventDestroy(s->fork);
   if (s->join) cudaEventDestroy(s->join);
+  if (s->fork0) cudaEventDestroy(s->fork0);
+  if (s->join0) cudaEventDestroy(s->join0);
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->mem) cudaFree(s->mem);
   for (int i = 0; i <= PL_STAGES; i++)

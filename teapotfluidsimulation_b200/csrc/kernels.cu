@@ -1016,6 +1016,15 @@ void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
 }
 
+// The cells' node partials, then the faces (k_p2g, this stream) and the density stage (k_density,
+// the second stream) side by side: both only read the partials, and they write disjoint arrays.
+void launch_p2g_cells(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+  k_p2g_cells<<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+}
+void launch_p2g_faces(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+  k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
+}
+
 void launch_stage_extrap(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_grad_ext1<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
   k_ext2<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);

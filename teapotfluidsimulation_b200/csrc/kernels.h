@@ -47,6 +47,9 @@ void launch_stage_density(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_stage_advect(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_pressure_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_correction_solve(const Geo& g, const DevPtrs& P, cudaStream_t st);
+// the two halves of the P2G stage, so that the density stage can run beside the faces
+void launch_p2g_cells(const Geo& g, const DevPtrs& P, cudaStream_t st);
+void launch_p2g_faces(const Geo& g, const DevPtrs& P, cudaStream_t st);
 // recording frames: every stride-th parcel's position quantised to u16 (format.ts:60)
 void launch_quantize(const DevPtrs& P, int n, int stride, double quantum, uint16_t* out, cudaStream_t st);
 struct PoissonImpl;
