@@ -373,10 +373,13 @@ int pl_pcg_solve_device(const uint8_t* cell, const double* b, double* q, int32_t
  * static device memory, one per device, sized for grids of up to PL_NOALLOC_MAX_CELLS cells
  * (about 30 MB); larger grids are rejected with PL_E_ARG. For hosts that own all device memory
  * (a pool or arena of their own, a budget that allows no allocation outside it) and so cannot
- * let a library call cudaMalloc/cudaFree. Runs on the current device; the first call on each
- * device looks up the scratch's device address (set-up), so make that first call before any
- * stream capture begins. Calls that overlap on one device (two host threads, or streams that
- * run at once) share the scratch and race: serialise them. Nothing has to be zeroed first. */
+ * let a library call cudaMalloc/cudaFree. Runs on the current device. Every call looks up the
+ * scratch's device address in the current context (no allocation); the first call in a context
+ * loads the library module that holds the scratch (set-up), so make that first call before any
+ * stream capture begins. The scratch stays with the device until the process exits; processes
+ * that never call this entry point do not hold it. Calls that overlap on one device (two host
+ * threads, or streams that run at once) share the scratch and race: serialise them. Nothing has
+ * to be zeroed first. */
 #define PL_NOALLOC_MAX_CELLS 262144
 int pl_pcg_solve_device_noalloc(const uint8_t* cell, const double* b, double* q, int32_t nx,
                                 int32_t ny, int32_t nz, double tol, int32_t max_iter, void* stream,

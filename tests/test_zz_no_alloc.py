@@ -1,8 +1,11 @@
 """pl_pcg_solve_device_noalloc against pl_pcg_solve_device, through the C ABI (needs a GPU).
 
-Both run the same MIC(0) FP64 kernels in the same order; the allocation-free call only takes its
-scratch from the library's fixed static device array. Tolerance: relative max difference 1e-12
-of the solution (the two are expected to agree bit for bit), equal iteration counts and residuals.
+The allocation-free entry point is for hosts that own all device memory and cannot let a library
+call cudaMalloc. Both calls run the same MIC(0) FP64 kernels in the same order; the allocation-free
+call only takes its scratch from the library's fixed static device array. Tolerance: relative max
+difference 1e-12 of the solution (the two are expected to agree bit for bit), equal iteration
+counts and residuals. This file is collected last, so a run that stops at the first failure has
+run every other test before it; it also passes alone in a fresh process.
 """
 import numpy as np
 import pytest
@@ -50,6 +53,29 @@ def test_noalloc_solve_matches_allocating_solve(engine, shape):
         assert np.abs(qn - want).max() <= TOL * scale
 
 
+def solve_both(engine, nx, ny, nz, seed, tol=1e-10, max_iter=400):
+    """One system solved by the allocating call and by the allocation-free call."""
+    import torch
+
+    cell, b = free_surface_system(nx, ny, nz, seed)
+    dc, db = torch.tensor(cell, device="cuda"), torch.tensor(b, device="cuda")
+    q_ref = torch.zeros(cell.size, dtype=torch.float64, device="cuda")
+    ref = engine.pcg_solve_device(dc.data_ptr(), db.data_ptr(), q_ref.data_ptr(), nx, ny, nz, tol, max_iter)
+    q = torch.full((cell.size,), float("nan"), dtype=torch.float64, device="cuda")
+    got = engine.pcg_solve_device_noalloc(dc.data_ptr(), db.data_ptr(), q.data_ptr(), nx, ny, nz, tol, max_iter)
+    return ref, q_ref.cpu().numpy(), got, q.cpu().numpy()
+
+
+def test_small_call_after_a_large_call_matches(engine):
+    # the scratch keeps the large call's contents; the small call that follows must not read any of it
+    for shape, seed in (((64, 64, 64), 5), ((9, 7, 5), 6), ((40, 32, 24), 7), ((11, 9, 6), 8)):
+        ref, want, got, qn = solve_both(engine, *shape, seed)
+        assert ref[1] and got[0] == ref[0] and got[1] == ref[1], (shape, ref, got)
+        assert abs(got[2] - ref[2]) <= TOL * max(abs(ref[2]), 1e-300)
+        assert np.isfinite(qn).all()
+        assert np.abs(qn - want).max() <= TOL * max(np.abs(want).max(), 1e-300), shape
+
+
 def test_noalloc_solve_rejects_grids_beyond_its_scratch(engine):
     import torch
 
@@ -60,9 +86,7 @@ def test_noalloc_solve_rejects_grids_beyond_its_scratch(engine):
     dq = torch.zeros_like(db)
     with pytest.raises(engine.EngineError, match="PL_NOALLOC_MAX_CELLS"):
         engine.pcg_solve_device_noalloc(dc.data_ptr(), db.data_ptr(), dq.data_ptr(), nx, ny, nz, 1e-10, 10)
-    # the rejection launched nothing; a valid call right after still works
-    cell, b = free_surface_system(9, 7, 5, seed=1)
-    dc, db = torch.tensor(cell, device="cuda"), torch.tensor(b, device="cuda")
-    dq = torch.zeros(cell.size, dtype=torch.float64, device="cuda")
-    _, conv, _ = engine.pcg_solve_device_noalloc(dc.data_ptr(), db.data_ptr(), dq.data_ptr(), 9, 7, 5, 1e-10, 200)
-    assert conv
+    # the rejection launched nothing; a valid call right after still works and matches
+    ref, want, got, qn = solve_both(engine, 9, 7, 5, seed=1)
+    assert got[1] and got[0] == ref[0]
+    assert np.abs(qn - want).max() <= TOL * max(np.abs(want).max(), 1e-300)
