@@ -1,6 +1,8 @@
 """Extract the golden vectors the tests pin the oracle and the engine against.
 
-Reads the reference's committed results (run with the reference mounted at /root/reference):
+Usage: python tests/golden/make_fixtures.py <reference checkout>
+
+Reads the reference's committed results from the given checkout:
   benchmarks/run3d.json      whole-pour results of the CPU solver at 5 and 4 mm
   benchmarks/gpu3d.json      the CPU state after 200 substeps at 5 mm (stepComparison.cpu)
   public/data/pour3d.bin.gz  the 5 mm recording (format: src/view3d/format.ts:4-8): origin tags
@@ -16,15 +18,17 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.dirname(os.path.abspath(__file__))
 FRAMES = [0, 2, 5, 9, 14, 19]  # within the first 1.9 s (the recording is 10 fps)
 
 
 def main():
-    run3d = json.load(open(os.path.join(REF, "benchmarks/run3d.json")))
-    gpu3d = json.load(open(os.path.join(REF, "benchmarks/gpu3d.json")))
-    raw = gzip.open(os.path.join(REF, "public/data/pour3d.bin.gz")).read()
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_fixtures.py <path of the reference checkout>")
+    ref = sys.argv[1]
+    run3d = json.load(open(os.path.join(ref, "benchmarks/run3d.json")))
+    gpu3d = json.load(open(os.path.join(ref, "benchmarks/gpu3d.json")))
+    raw = gzip.open(os.path.join(ref, "public/data/pour3d.bin.gz")).read()
     hl = struct.unpack("<I", raw[:4])[0]
     head = json.loads(raw[4:4 + hl])
     P = head["parcels"]
