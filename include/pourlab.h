@@ -289,10 +289,24 @@ enum pl_stage {
   PL_STAGE_ADVECT = 6,   /* grid-to-particle, advection, collisions, accounting */
   PL_STAGES = 7
 };
-/* Record CUDA events between the stages of every substep (rebuilds the substep graph). */
+/* Record CUDA events between the stages of every substep (rebuilds the substep graph). The
+ * density stage runs on a second stream beside the P2G face pass: its interval overlaps
+ * PL_STAGE_P2G, which ends when both are done. The six other stages add up to the substep. */
 int pl_enable_stage_timing(pl_sim* sim, int32_t on);
 /* Device milliseconds per stage of the last completed substep (needs stage timing on). */
 int pl_stage_times(pl_sim* sim, float ms[PL_STAGES]);
+
+/* Host-side failure injection for tests (no counterpart in the solver; the reference injects
+ * readback failures into its fake GPU, tests/fakeGpu.ts:26-33). PL_FAULT_ALLOC: the next `count`
+ * device allocations of pl_create on this host thread fail as an out-of-memory cudaMalloc would
+ * (pl_create returns PL_E_NOMEM and frees what it had set up); count 0 clears it. */
+#define PL_FAULT_ALLOC 1
+int pl_inject_fault(int32_t kind, int32_t count);
+/* Polls before the binning scan's bounded look-back wait gives up (0: the default, 2^22). A wait
+ * that gives up switches the rest of the substep off (the parcels keep their state) and the call
+ * that synchronises reports PL_E_TIMEOUT; the handle stays in that error. For tests of the
+ * bounded-wait path (no counterpart in the reference). */
+int pl_set_wait_limit(pl_sim* sim, int32_t polls);
 /* Launch-shape tuner of the cluster solves (no counterpart in the reference): runs `substeps`
  * substeps of cfg from its initial state for every candidate (cluster CTAs x threads per CTA) on a
  * scratch simulation and returns the shape with the smallest pressure + correction time, and that
@@ -404,7 +418,8 @@ enum pl_poisson_method {
  * liquid spheres (radius 6-24 cells at n = 128) from mulberry32 (src/sim/rng.ts:5-14) seeded 1000 +
  * snapshot, AIR elsewhere; rhs = -div of a unit-variance Gaussian random face-velocity field
  * (standard deviation 8 cells at n = 128) on the unknowns, with the gauge fix applied. threads <= 0:
- * all hardware threads. cell: count * n^3 bytes, b: count * n^3 floats. */
+ * all hardware threads. cell: count * n^3 bytes, b: count * n^3 floats, or NULL for the masks alone
+ * (no rhs and no gauge fix: the cheap part, whose unknowns give a snapshot's cost for sharding). */
 int pl_poisson_generate(int32_t n, int32_t first, int32_t count, uint8_t* cell, float* b, int32_t threads);
 /* The gauge fix on caller cells and rhs (host arrays, count snapshots of n^3): every 6-connected
  * component of unknowns without an AIR neighbour gets its rhs mean removed and its first cell (index

@@ -642,13 +642,18 @@ struct plo_sim {
     for (int p = 0; p < n; p++) {
       if (status[p] != IN_POT) continue;
       double fi = std::floor(x[p] / h), fj = std::floor(y[p] / h), fk = std::floor(z[p] / h);
+      if (std::isnan(fi + fj + fk)) continue;  // cell[NaN] reads undefined in JavaScript: no-op
       if (fi < 1 || fj < 1 || fk < 1 || fi >= nx - 1 || fj >= ny - 1 || fk >= nz - 1) continue;
       size_t c = size_t(fi) + size_t(nx) * (size_t(fj) + size_t(ny) * size_t(fk));
       if (cell[c] == AIR) cell[c] = FLUID;
     }
   }
 
-  // solver3d.ts:339-362
+  // A stencil of a NaN position: every corner index is NaN in the reference, and a typed array indexed
+  // with NaN reads undefined (NaN in arithmetic, falsy as a mask) and ignores writes.
+  static constexpr size_t NAN_INDEX = ~size_t(0);
+
+  // solver3d.ts:339-362 (NAN_INDEX when a coordinate is NaN)
   size_t stencil(double px, double py, double pz, double ox, double oy, double oz, int sx, int sy, int sz,
                  double* out) const {
     double gx = px / h - ox, gy = py / h - oy, gz = pz / h - oz;
@@ -658,6 +663,7 @@ struct plo_sim {
     out[0] = js_max(0, js_min(1, gx - i));
     out[1] = js_max(0, js_min(1, gy - j));
     out[2] = js_max(0, js_min(1, gz - k));
+    if (std::isnan(i + j + k)) return NAN_INDEX;
     return size_t(i) + size_t(sx) * (size_t(j) + size_t(sy) * size_t(k));
   }
 
@@ -693,6 +699,7 @@ struct plo_sim {
     int sz[3];
     dims(comp, o, sz);
     size_t base = stencil(px, py, pz, o[0], o[1], o[2], sz[0], sz[1], sz[2], st);
+    if (base == NAN_INDEX) return NAN;  // all = NaN, ws = 0
     double acc = 0, ws = 0, all = 0;
     forEachCorner(base, sz[0], sz[1], [&](size_t idx, double wgt) {
       all += wgt * field[idx];
@@ -720,6 +727,7 @@ struct plo_sim {
       for (int p = 0; p < n; p++) {
         if (status[p] != IN_POT) continue;
         size_t base = stencil(x[p], y[p], z[p], o[0], o[1], o[2], sz[0], sz[1], sz[2], st);
+        if (base == NAN_INDEX) continue;  // writes to NaN indices are ignored
         double vp = vel[p];
         if (apic) {  // affine field at each corner face (src/sim/solver.ts:553-587 in 3D)
           const size_t sxy = size_t(sz[0]) * sz[1];
@@ -907,6 +915,10 @@ struct plo_sim {
     int sz[3];
     dims(comp, o, sz);
     size_t base = stencil(px, py, pz, o[0], o[1], o[2], sz[0], sz[1], sz[2], st);
+    if (base == NAN_INDEX) {
+      g3[0] = g3[1] = g3[2] = NAN;
+      return;
+    }
     const size_t sx = size_t(sz[0]), sxy = size_t(sz[0]) * sz[1];
     double u[8];
     for (int c = 0; c < 8; c++) u[c] = field[base + (c & 1) + ((c & 2) ? sx : 0) + ((c & 4) ? sxy : 0)];
@@ -961,6 +973,7 @@ struct plo_sim {
     for (int p = 0; p < n; p++) {
       if (status[p] != IN_POT) continue;
       size_t base = stencil(x[p], y[p], z[p], 0.5, 0.5, 0.5, nx, ny, nz, ds);
+      if (base == NAN_INDEX) continue;
       st[0] = ds[0], st[1] = ds[1], st[2] = ds[2];
       forEachCorner(base, nx, ny, [&](size_t idx, double wgt) { density[idx] += wgt; });
     }

@@ -95,7 +95,7 @@ struct SimScalars {
   double forced_dt; // > 0: dt of the forced substep; else the stable dt
   // this substep
   int active;
-  int pad0;
+  int spin_limit;  // polls before the bin scan's bounded look-back wait gives up (0: SPIN_LIMIT)
   double dt, phi1;
   double c0, s0, c1, s1;
   // counters (integer: order-independent, deterministic)

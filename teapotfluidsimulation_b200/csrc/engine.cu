@@ -26,6 +26,7 @@ using namespace pl;
 namespace {
 
 thread_local std::string g_err;
+thread_local int g_fail_allocs = 0;  // pl_inject_fault(PL_FAULT_ALLOC, n): pl_create allocations left to fail
 
 int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 int fail(int code, const char* fmt, ...) {
@@ -65,7 +66,8 @@ struct pl_sim {
   SimScalars* pinned = nullptr; // page-locked staging of the scalar block
   int timing = 0;
   int pending = 0;  // substeps queued by pl_enqueue_substeps since the last pull
-  cudaEvent_t ev[PL_STAGES + 1] = {};
+  int free_running = 0;  // the device's control fields already say "run until finished" (no copy needed)
+  cudaEvent_t ev[PL_STAGES + 3] = {};  // stage boundaries on st (0-7) and the density branch on st2 (8-9)
   pl::PoissonImpl* box = nullptr;  // grid-scale solver (PL_PRECOND_BOX_MG / PL_PRECOND_LEARNED)
   pl::PoissonImpl* box2 = nullptr; // ... and the density correction's (multigrid), run beside it
   cudaStream_t st2 = nullptr;      // the second stream of the substep capture
@@ -96,6 +98,7 @@ int pull_scalars(pl_sim* s) {
 }
 
 int push_scalars(pl_sim* s) {
+  s->free_running = 0;
   std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
   CK(cudaMemcpyAsync(s->P.sc, s->pinned, sizeof(SimScalars), cudaMemcpyHostToDevice, s->st));
   CK(cudaStreamSynchronize(s->st));
@@ -108,9 +111,10 @@ int record_substep(pl_sim* s) {
   const Geo& g = s->g;
   const DevPtrs& P = s->P;
   cudaStream_t st = s->st;
-  auto mark = [&](int i) {  // external: becomes an event-record node of the captured graph
-    if (s->timing) cudaEventRecordWithFlags(s->ev[i], st, cudaEventRecordExternal);
+  auto mark_on = [&](int i, cudaStream_t on) {  // external: becomes an event-record node of the captured graph
+    if (s->timing) cudaEventRecordWithFlags(s->ev[i], on, cudaEventRecordExternal);
   };
+  auto mark = [&](int i) { mark_on(i, st); };
   // execution order: bin, p2g, density, pressure, correction, extrapolation, advect (the density
   // stage needs only the parcels and cell types, so it runs before the solves)
   mark(0);
@@ -121,7 +125,9 @@ int record_substep(pl_sim* s) {
   launch_p2g_cells(g, P, st);
   cudaEventRecord(s->fork0, st);
   cudaStreamWaitEvent(s->st2, s->fork0, 0);
+  mark_on(8, s->st2);
   launch_stage_density(g, P, s->st2);
+  mark_on(9, s->st2);
   cudaEventRecord(s->join0, s->st2);
   launch_p2g_faces(g, P, st);
   mark(2);
@@ -144,8 +150,11 @@ int record_substep(pl_sim* s) {
   return PL_OK;
 }
 
-// Event interval [first, second] of each stage (enum pl_stage order) in the execution order above.
-const int kStageEvents[PL_STAGES][2] = {{0, 1}, {1, 2}, {3, 4}, {5, 6}, {2, 3}, {4, 5}, {6, 7}};
+// Event interval [first, second] of each stage (enum pl_stage order) in the execution order above. P2G
+// ends when both its face pass and the density branch beside it are done; the density stage is its
+// own branch's interval on the second stream, which overlaps P2G. The six other stages tile the
+// substep.
+const int kStageEvents[PL_STAGES][2] = {{0, 1}, {1, 3}, {3, 4}, {5, 6}, {8, 9}, {4, 5}, {6, 7}};
 
 int build_graph(pl_sim* s) {
   if (s->exec) {
@@ -291,7 +300,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->fork0, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->join0, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&s->pinned, sizeof(SimScalars), cudaHostAllocDefault);
-  for (int i = 0; i <= PL_STAGES && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
+  for (int i = 0; i < PL_STAGES + 3 && e == cudaSuccess; i++) e = cudaEventCreate(&s->ev[i]);
   if (e != cudaSuccess) {
     pl_destroy(s);
     return fail(PL_E_CUDA, "pl_create: stream, events or pinned staging: %s", cudaGetErrorString(e));
@@ -322,7 +331,12 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
-  e = cudaMalloc(&s->mem, total);
+  if (g_fail_allocs > 0) {  // injected: the allocation fails as cudaMalloc reports running out of memory
+    g_fail_allocs--;
+    e = cudaErrorMemoryAllocation;
+  } else {
+    e = cudaMalloc(&s->mem, total);
+  }
   if (e != cudaSuccess) {
     pl_destroy(s);
     return fail(PL_E_NOMEM, "cudaMalloc(%zu): %s", total, cudaGetErrorString(e));
@@ -469,7 +483,7 @@ void pl_destroy(pl_sim* s) {
   if (s->join0) cudaEventDestroy(s->join0);
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->mem) cudaFree(s->mem);
-  for (int i = 0; i <= PL_STAGES; i++)
+  for (int i = 0; i < PL_STAGES + 3; i++)
     if (s->ev[i]) cudaEventDestroy(s->ev[i]);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->st) cudaStreamDestroy(s->st);
@@ -482,11 +496,15 @@ int pl_enqueue_substeps(pl_sim* s, int32_t count) {
   cudaSetDevice(s->device);
   s->hs.end_time = INFINITY;  // run until finished
   s->hs.force_step = 0;
-  std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
-  // only the control fields change: copy end_time .. forced_dt
-  const size_t off = offsetof(SimScalars, end_time);
-  const size_t len = offsetof(SimScalars, active) - off;
-  CK(cudaMemcpyAsync((char*)s->P.sc + off, (char*)s->pinned + off, len, cudaMemcpyHostToDevice, s->st));
+  if (!s->free_running) {
+    // only the control fields change: copy end_time .. forced_dt (once; the substeps leave them as
+    // they are, so later calls launch the graph alone until a call pushes the scalar block again)
+    std::memcpy(s->pinned, &s->hs, sizeof(SimScalars));
+    const size_t off = offsetof(SimScalars, end_time);
+    const size_t len = offsetof(SimScalars, active) - off;
+    CK(cudaMemcpyAsync((char*)s->P.sc + off, (char*)s->pinned + off, len, cudaMemcpyHostToDevice, s->st));
+    s->free_running = 1;
+  }
   for (int i = 0; i < count; i++) CK(cudaGraphLaunch(s->exec, s->st));
   s->pending = 1;
   return PL_OK;
@@ -536,6 +554,21 @@ int pl_autotune_solver(const pl_config* cfg, int32_t substeps, int32_t* best_clu
   *best_threads = bt;
   if (best_ms) *best_ms = best;
   return PL_OK;
+}
+
+int pl_inject_fault(int32_t kind, int32_t count) {
+  if (kind != PL_FAULT_ALLOC || count < 0) return fail(PL_E_ARG, "pl_inject_fault: unknown fault %d or count %d", kind, count);
+  g_fail_allocs = count;
+  return PL_OK;
+}
+
+int pl_set_wait_limit(pl_sim* s, int32_t polls) {
+  if (!s || polls < 0) return fail(PL_E_ARG, "pl_set_wait_limit: bad argument");
+  cudaSetDevice(s->device);
+  int rc = settle(s);
+  if (rc) return rc;
+  s->hs.spin_limit = polls;
+  return push_scalars(s);
 }
 
 int pl_enable_stage_timing(pl_sim* s, int32_t on) {
@@ -880,7 +913,7 @@ int pl_set_state(pl_sim* s, const pl_sim_state* st, const double* x, const doubl
       if (status[p] == PL_DISCHARGED) h.by_origin[s->origin[p]]++;
       if (status[p] == PL_IN_POT && vx && vy && vz) {
         double a = (float)vx[p], b = (float)vy[p], c = (float)vz[p];
-        double sp = a * a + b * b + c * c;
+        double sp = a * a + b * b + c * c;  // as k_advect forms it (no contraction: -ffp-contract=off)
         if (sp > m) m = sp;
       }
     }
@@ -999,7 +1032,7 @@ struct pl_poisson {
 };
 
 int pl_poisson_generate(int32_t n, int32_t first, int32_t count, uint8_t* cell, float* b, int32_t threads) {
-  if (!cell || !b) return fail(PL_E_ARG, "pl_poisson_generate: null buffer");
+  if (!cell) return fail(PL_E_ARG, "pl_poisson_generate: null buffer");
   if (n < 8 || n > 512 || (n & (n - 1)) || count < 1 || first < 0)
     return fail(PL_E_ARG, "pl_poisson_generate: n must be a power of two in [8, 512] and count >= 1 (n=%d count=%d)",
                 n, count);

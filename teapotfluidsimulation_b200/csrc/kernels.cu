@@ -121,7 +121,10 @@ __global__ void k_bin_count(Geo g, DevPtrs P) {
   int status = __float_as_int(v.w) & 0xff;
   int id = __float_as_int(p.w);
   int key;
-  if (status == IN_POT) {
+  // A non-finite in-pot parcel is in no cell: the reference's classify and particle-to-grid index its
+  // typed arrays with NaN, which reads undefined and writes nothing (solver3d.ts:329-335, 339-431);
+  // advection then marks it LOST (solver3d.ts:761-764). It waits in a removed-parcel bin.
+  if (status == IN_POT && isfinite(p.x + p.y + p.z)) {
     float4 fr;
     int outl;
     key = parcel_bin(g, p, &fr, &outl);
@@ -217,6 +220,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       unsigned long long excl = 0;
       int top = tile - 1;  // highest predecessor not yet summed
       int spins = 0;
+      const int limit = sc->spin_limit > 0 ? sc->spin_limit : SPIN_LIMIT;
       bool failed = false;
       while (top >= 0) {
         const int j = top - lane;
@@ -227,7 +231,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
         const int first = inc ? __ffs(inc) - 1 : 31;
         const unsigned need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
         if (pend & need) {  // a needed descriptor is not published yet
-          if (++spins > SPIN_LIMIT) {
+          if (++spins > limit) {
             failed = true;
             break;
           }
@@ -274,6 +278,13 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
 __global__ void k_bin_place(Geo g, DevPtrs P) {
   if (!P.sc->active) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
+  // A look-back that gave up left partial bin starts (each at most the true start, so every write of
+  // the scan stayed in bounds). Nothing after it may use them: the substep is switched off here, every
+  // later kernel returns at its active check, and the parcels keep their state before the substep.
+  if (P.sc->errors & ERR_SCAN_TIMEOUT) {
+    if (s == 0) P.sc->active = 0;
+    return;
+  }
   if (s >= g.n) return;
   int key = P.key[s];
   int id = __float_as_int(P.pos_home[s].w);
@@ -710,9 +721,12 @@ __device__ __forceinline__ Sten face_stencil(const Geo& g, int comp, double x, d
   double ox = comp == 0 ? 0.0 : 0.5, oy = comp == 1 ? 0.0 : 0.5, oz = comp == 2 ? 0.0 : 0.5;
   int sx = g.nx + (comp == 0), sy = g.ny + (comp == 1), sz = g.nz + (comp == 2);
   double gx = x / g.h - ox, gy = y / g.h - oy, gz = z / g.h - oz;
-  double i = dmax(0.0, dmin((double)(sx - 2), floor(gx)));
-  double j = dmax(0.0, dmin((double)(sy - 2), floor(gy)));
-  double k = dmax(0.0, dmin((double)(sz - 2), floor(gz)));
+  // clamp(floor(g), 0, s - 2); a NaN coordinate clamps to 0, so no index is ever formed from a NaN
+  // (its weights stay NaN and the sample is NaN, as the reference's is)
+  auto clampi = [](double f, int hi) { return f >= 0.0 ? (f <= (double)hi ? f : (double)hi) : 0.0; };
+  double i = clampi(floor(gx), sx - 2);
+  double j = clampi(floor(gy), sy - 2);
+  double k = clampi(floor(gz), sz - 2);
   Sten s;
   s.fx = dmax(0.0, dmin(1.0, gx - i));
   s.fy = dmax(0.0, dmin(1.0, gy - j));
@@ -943,7 +957,10 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
     if (new_st == DISCHARGED) atomicAdd(&sc->by_origin[(meta >> 8) & 0xff], 1);
     vel.w = __int_as_float((meta & ~0xff) | new_st);
   } else {
-    const double sp = vx * vx + vy * vy + vz * vz;  // stableDt (solver3d.ts:269-274) of the next substep
+    // stableDt (solver3d.ts:269-274) of the next substep, from the velocity as stored: a state saved
+    // now and restored (pl_set_state recounts it the same way) continues with the same dt
+    const double fx = vel.x, fy = vel.y, fz = vel.z;
+    const double sp = DADD(DADD(DMUL(fx, fx), DMUL(fy, fy)), DMUL(fz, fz));
     P.pos_home[p] = pos;
     P.vel_home[p] = vel;
     return (unsigned long long)__double_as_longlong(sp);

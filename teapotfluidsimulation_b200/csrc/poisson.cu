@@ -1391,6 +1391,7 @@ void generate_one(int n, int snapshot, uint8_t* cell, float* bout) {
         }
         cell[c] = t;
       }
+  if (!bout) return;  // the mask alone (its unknowns give the snapshot's cost for sharding)
   // Gaussian random face velocities: white noise smoothed by a separable Gaussian of standard
   // deviation 8 cells (at n = 128; scaled with n), unit variance; rhs = -div on the unknowns.
   const double sig = 8.0 * sc;
@@ -1515,7 +1516,8 @@ int poisson_generate(int n, int first, int count, uint8_t* cell, float* b, int t
   std::vector<std::thread> pool;
   for (int t = 0; t < threads; t++)
     pool.emplace_back([=]() {
-      for (int s = t; s < count; s += threads) generate_one(n, first + s, cell + size_t(s) * nc, b + size_t(s) * nc);
+      for (int s = t; s < count; s += threads)
+        generate_one(n, first + s, cell + size_t(s) * nc, b ? b + size_t(s) * nc : nullptr);
     });
   for (auto& th : pool) th.join();
   return PL_OK;

@@ -32,6 +32,7 @@ EXPORTED = [
     "pl_unet_set_params", "pl_unet_apply", "pl_unet_train_step", "pl_unet_gradient", "pl_unet_destroy",
     "pl_unet_set_loss", "pl_set_unet", "pl_unet_set_conv_kernel", "pl_unet_error", "pl_read_quantized_positions", "pl_ensemble_configs", "pl_ensemble_create", "pl_ensemble_size",
     "pl_ensemble_member", "pl_ensemble_advance", "pl_ensemble_enqueue", "pl_ensemble_destroy",
+    "pl_inject_fault", "pl_set_wait_limit",
     "pl_poisson_generate", "pl_poisson_gauge_fix", "pl_poisson_create", "pl_poisson_create_box", "pl_poisson_set_unet", "pl_poisson_solve", "pl_poisson_device_bytes", "pl_poisson_history", "pl_poisson_destroy",
 ]
 STAGES = ["bin", "p2g", "pressure", "extrap", "density", "correction", "advect"]
@@ -96,6 +97,8 @@ def lib() -> C.CDLL:
     L.pl_stream.restype = C.c_void_p
     L.pl_enable_stage_timing.argtypes = [P, C.c_int32]
     L.pl_stage_times.argtypes = [P, fp]
+    L.pl_inject_fault.argtypes = [C.c_int32, C.c_int32]
+    L.pl_set_wait_limit.argtypes = [P, C.c_int32]
     L.pl_unet_create.argtypes = [C.c_uint32, C.POINTER(P)]
     L.pl_unet_num_params.argtypes = [P]
     L.pl_unet_num_params.restype = C.c_int32
@@ -275,6 +278,10 @@ class Simulation3D:
         _check(lib().pl_stage_times(self._h, _ptr(out, C.c_float)))
         return dict(zip(STAGES, out.tolist()))
 
+    def set_wait_limit(self, polls: int):
+        """Polls before the bin scan's bounded look-back wait gives up (0: the default); for tests."""
+        _check(lib().pl_set_wait_limit(self._h, int(polls)))
+
     # ------------------------------------------------------------ controller
     def set_target(self, angle_deg: float, time: float | None = None):
         """controller.setTarget(angleDeg, time) (src/sim/motion.ts:40-44): the setTilt of a manual pour."""
@@ -379,6 +386,15 @@ class Simulation3D:
         out = np.zeros(n, dtype)
         _check(lib().pl_get_field(self._h, which, out.ctypes.data_as(C.c_void_p), n))
         return out
+
+
+FAULT_ALLOC = 1  # PL_FAULT_ALLOC
+
+
+def inject_fault(kind: int, count: int = 1):
+    """Host-side failure injection (pl_inject_fault): the next `count` device allocations of
+    pl_create on this thread fail as an out-of-memory cudaMalloc would."""
+    _check(lib().pl_inject_fault(int(kind), int(count)))
 
 
 def pcg_solve_device(cell_ptr: int, b_ptr: int, q_ptr: int, nx: int, ny: int, nz: int, tol: float, max_iter: int,
