@@ -1,25 +1,33 @@
 """Benchmark of the B200 pour engine: simulated seconds per wall second of the 4 mm gentle pour.
 
 One step is one substep of the pour (binning, particle-to-grid, pressure solve, extrapolation,
-density correction, advection). The timed region runs K substeps after W warm-up substeps, each
-substep timed on the engine's stream with CUDA events (the graph's first and last stage events),
-with a 256 MiB buffer written between substeps so every substep starts with a cold L2. The
-reported value is the simulated time those K substeps covered divided by their summed device time.
+density correction, advection). The timed region runs K substeps after W warm-up substeps, from a
+mid-pour state (by default 3 s into the pour: the pot tilted, liquid in the spout), each substep one
+launch of the production substep graph bracketed by CUDA events on the engine's stream, with a
+256 MiB buffer written before each substep (outside the bracket) so every substep starts with a cold
+L2. The reported value is the simulated time those K substeps covered divided by their summed
+device time. The per-stage split comes from a second replica from the same start whose graph holds
+stage events.
 
 `e2e` repeats the measurement through the public C ABI call a host program makes per substep
 (pl_step: host->device control block, the substep, device->host stats block), timed by the host
-clock around each call. The reference arm (--impl reference) times the CPU FP64 restatement of the
-reference solver on the same workload (the reference itself is TypeScript and no JavaScript
+clock around each call. `whole_pour` runs the reference's own benchmark loop (benchmarks/run3d.ts:
+the whole pour until 1.5 s after the controller is done, pl_advance in 0.5 s chunks) with the
+Chebyshev and the multigrid preconditioner, and compares the poured volume and layer shares with the
+reference CPU solver's result. The reference arm (--impl reference) times the CPU FP64 restatement of
+the reference solver on the same workload (the reference itself is TypeScript and no JavaScript
 runtime exists on the box).
 
-A second, supplementary measurement (`poisson_batch` in the same line) solves the isolated
-pressure-Poisson batch (64 snapshots of 128^3 per GPU) with multigrid- and MIC(0)-preconditioned CG,
-each timed with CUDA events around the public pl_poisson_solve call on inputs resident in HBM (671 MB,
-larger than L2), beside the CPU FP64 oracle on a bounded sample.
+Supplementary measurements in the same line: `poisson_batch` solves the isolated pressure-Poisson
+batch (64 snapshots of 128^3 per GPU) with multigrid- and MIC(0)-preconditioned CG, each timed with
+CUDA events around the public pl_poisson_solve call on inputs resident in HBM (671 MB, larger than
+L2), beside the CPU FP64 oracle on a bounded sample; `full_domain` and `ensemble` time the 2.5 mm
+full-domain APIC pour and the 256-pour ensemble.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU: torchrun --nproc-per-node N bench.py --gpus N: every rank runs its own replica of the
-pour (the single pour does not shard); value is the sum over ranks, timed as the max over ranks.
+pour (the single pour does not shard); value is the sum over ranks, timed as the max over ranks. The
+Poisson batch and the ensemble are partitioned over the ranks by estimated cost.
 """
 from __future__ import annotations
 
@@ -56,7 +64,10 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["f64", "mixed"],
                     help="solver vectors: mixed = FP32 stencils/Chebyshev with FP64 inner products and FP64 "
                          "true-residual refinement; f64 = all FP64")
-    ap.add_argument("--start", type=float, default=0.0, help="simulated seconds to advance before warm-up")
+    ap.add_argument("--start", type=float, default=3.0,
+                    help="simulated seconds to advance before warm-up (3 s: the pot tilted, liquid in the spout)")
+    ap.add_argument("--whole-pour", type=int, default=1,
+                    help="1: also time the whole pour (run3d.ts rule) with Chebyshev and multigrid PCG")
     ap.add_argument("--cpu-sample", type=int, default=60, help="substeps of the CPU baseline sample")
     ap.add_argument("--poisson-n", type=int, default=128, help="grid of the isolated Poisson batch (0: skip it)")
     ap.add_argument("--poisson-count", type=int, default=64, help="snapshots of the isolated Poisson batch per GPU")
@@ -255,9 +266,18 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
     from teapotfluidsimulation_b200 import abi
     from teapotfluidsimulation_b200 import engine as E
 
-    n, count = args.poisson_n, args.poisson_count
+    from teapotfluidsimulation_b200 import sharding
+
+    n = args.poisson_n
     t0 = time.perf_counter()
-    cell, b = E.poisson_generate(n, poisson_first_snapshot(rank, count), count)
+    mine = shard_snapshots(n, args.poisson_count * world, rank, world)
+    count = len(mine)
+    cell = np.zeros((count, n ** 3), np.uint8)
+    b = np.zeros((count, n ** 3), np.float32)
+    at = 0
+    for first, k in sharding.contiguous_runs(mine):
+        cell[at:at + k], b[at:at + k] = E.poisson_generate(n, first, k)
+        at += k
     gen_s = time.perf_counter() - t0
     m_each = ((cell & 3) == abi.FLUID).sum(axis=1)  # unknowns per snapshot (border cells are SOLID)
     dc = torch.from_numpy(cell).cuda()
@@ -284,8 +304,10 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
     ref, (ref_ms, ref_it, ref_conv), _ = solve(E.POISSON_MG, abi.SOLVE_F64, 1e-12, 1)
     refn = ref.abs().amax(dim=1).clamp_min(1e-300)
     peaks, peak_kind = measured_peaks()
-    out = {"workload": f"{count} snapshots of {n}^3 per GPU (cylinder wall, slab, 1-8 mulberry32 spheres; "
-                       f"rhs = -div of a Gaussian random face field), seeds {1000 + rank * count}..",
+    out = {"workload": f"{args.poisson_count} snapshots of {n}^3 per GPU (cylinder wall, slab, 1-8 mulberry32 "
+                       f"spheres; rhs = -div of a Gaussian random face field), seeds 1000.."
+                       f"{1000 + args.poisson_count * world - 1}, partitioned over ranks by unknowns",
+           "snapshots_this_rank": count,
            "unknowns": int(m_each.sum()), "generate_s": gen_s, "tolerance": "max|r| <= 1e-6 max|b|",
            "reference": {"method": "MG-PCG FP64 to 1e-12 (GPU; pinned to the CPU FP64 oracle in the tests)",
                          "ms": ref_ms, "iterations_mean": float(ref_it.mean()), "converged": bool(ref_conv.all())}}
@@ -298,7 +320,7 @@ def run_poisson(args, world: int, rank: int) -> dict | None:
         work = float(sum(per_it(int(m)) * int(k) for m, k in zip(m_each, it)))
         achieved = work / (ms / 1e3) / 1e9
         out[name] = {"ms_per_batch": ms_max, "ms_per_snapshot": ms_max / count,
-                     "snapshots_per_s": allsum(count, world) / (ms_max / 1e3),
+                     "snapshots_per_s": args.poisson_count * world / (ms_max / 1e3),
                      "iterations_mean": float(it.mean()), "iterations_max": int(it.max()),
                      "converged": bool(conv.all()), "max_rel_err_vs_fp64_1e-12": err, "device_gb": dev_bytes / 1e9,
                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
@@ -389,7 +411,7 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
             its.append(d["pressureIterations"])
             cits.append(d["correctionIterations"])
         d1 = sim.diagnostics()
-        ms = allmax(sum(acc.values()), world)
+        ms = allmax(sum(v for name, v in acc.items() if name != "density"), world)  # density overlaps P2G
         return {"substeps": k, "ms_per_substep": ms / k,
                 "sim_s_per_wall_s": allsum(d1["time"] - d0["time"], world) / (ms / 1e3),
                 "pressure_ms_per_substep": acc["pressure"] / k, "correction_ms_per_substep": acc["correction"] / k,
@@ -440,15 +462,24 @@ def run_full_domain(args, world: int, rank: int) -> dict | None:
     return out
 
 
-def shard_pours(items: list, rank: int, world: int) -> list:
-    """The pours of an ensemble this rank runs: round-robin over the ranks (no collective on the data
-    path; every pour on exactly one rank)."""
-    return items[rank::world]
+def shard_pours(cfgs: list, rank: int, world: int) -> list[int]:
+    """Indices of the ensemble's pours this rank runs: a partition by estimated cost (cells + parcels times
+    estimated substeps), the same on every rank without communication; no collective on the data path."""
+    from teapotfluidsimulation_b200 import sharding
+
+    if world == 1:
+        return list(range(len(cfgs)))
+    return sharding.partition_by_cost(sharding.pour_costs(cfgs), world)[rank]
 
 
-def poisson_first_snapshot(rank: int, count: int) -> int:
-    """First snapshot index (seed offset) of this rank's share of the Poisson batch."""
-    return rank * count
+def shard_snapshots(n: int, total: int, rank: int, world: int) -> list[int]:
+    """Snapshot indices of the Poisson batch this rank solves: a partition of all ranks' snapshots by their
+    unknowns (masks generated on every rank, cheap: no rhs)."""
+    from teapotfluidsimulation_b200 import sharding
+
+    if world == 1:
+        return list(range(total))
+    return sharding.partition_by_cost(sharding.snapshot_costs(n, 0, total), world)[rank]
 
 
 def run_ensemble(args, world: int, rank: int) -> dict | None:
@@ -463,8 +494,11 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
     from teapotfluidsimulation_b200 import abi
     from teapotfluidsimulation_b200 import engine as E
 
+    from teapotfluidsimulation_b200 import sharding
+
     cfgs = E.ensemble_configs(2026, args.ensemble_count, args.ensemble_mm, 20.0)
-    mine = shard_pours(cfgs, rank, world)
+    mine_idx = shard_pours(cfgs, rank, world)
+    mine = [cfgs[i] for i in mine_idx]
     for c in mine:
         c.preconditioner = abi.PRECOND_CHEB
         c.solve_precision = abi.SOLVE_MIXED
@@ -487,6 +521,13 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
     wall = allmax(time.perf_counter() - t0, world)
     sim_s = sum(m.diagnostics()["time"] - t for m, t in zip(ens.members, t_before))
     fails = sum(m.diagnostics()["pressureFailures"] for m in ens.members)
+    # per-pour stats (about a hundred bytes each), gathered from every rank
+    local = {}
+    for i, m in zip(mine_idx, ens.members):
+        d = m.diagnostics()
+        local[i] = {"time": d["time"], "steps": d["steps"], "discharged_ml": d["dischargedMl"],
+                    "pressure_failures": d["pressureFailures"], "cells": m.nx * m.ny * m.nz}
+    stats = sharding.gather_stats(local, world)
     # the same kind of work one pour at a time (the first few pours), for the concurrency gain
     seq_wall, seq_sim = 0.0, 0.0
     for m in ens.members[: min(8, len(ens.members))]:
@@ -505,17 +546,23 @@ def run_ensemble(args, world: int, rank: int) -> dict | None:
             "cells_min": min(grids), "cells_max": max(grids), "create_s": create_s,
             "sim_s_per_wall_s": total_sim / wall, "pour_substeps_per_s": allsum(len(mine), world) * args.ensemble_steps / wall,
             "wall_s": wall, "pressure_failures": fails,
+            "pours_gathered": len(stats), "cells_total": sum(v["cells"] for v in stats.values()),
+            "sharding": "pours partitioned by estimated cost (cells + parcels) x substeps; stats gathered "
+                        "from every rank",
             "one_at_a_time_sim_s_per_wall_s": seq_sim / seq_wall if seq_wall > 0 else None,
             "concurrency_gain": (sim_s / wall) / (seq_sim / seq_wall) if seq_wall > 0 and seq_sim > 0 else None,
             "timing": "host clock around the interleaved launches and every pour's synchronisation"}
 
 
-def run_cpu_baseline(args, substeps: int) -> dict:
-    """The CPU FP64 restatement of the reference solver on a bounded sample of the same workload."""
+def run_cpu_baseline(args, substeps: int, state=None) -> dict:
+    """The CPU FP64 restatement of the reference solver on a bounded sample of the same workload, from
+    the engine's state at the start of the timed window when one is given."""
     from oracle import oracle as O
 
     sim = O.OracleSim(make_cfg(args))
-    if args.start > 0:
+    if state is not None:
+        sim.set_state(*state)
+    elif args.start > 0:
         sim.advance(args.start)
     t_sim0 = sim.diagnostics()["time"]
     t0 = time.perf_counter()
@@ -525,9 +572,100 @@ def run_cpu_baseline(args, substeps: int) -> dict:
     t_sim = sim.diagnostics()["time"] - t_sim0
     sim.close()
     return {"value": t_sim / wall, "unit": "sim-s/wall-s", "cores": 1, "kind": "port",
-            "sample": f"{substeps} substeps of the same pour from t={args.start:g} s, C++ FP64 restatement "
+            "sample": f"{substeps} substeps of the same pour from t={t_sim0:.3f} s, C++ FP64 restatement "
                       f"of src/sim3d (one thread; the reference is single-threaded TypeScript)",
             "wall_s": wall, "sim_s": t_sim, "ms_per_substep": 1000 * wall / substeps}
+
+
+def reference_pour_result(cell_mm: float) -> dict | None:
+    """The reference CPU solver's whole-pour result at this cell size (benchmarks/run3d.json, committed
+    as a test fixture)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "reference_goldens.json")) as f:
+            rows = json.load(f)["run3d"]
+    except (OSError, KeyError):
+        return None
+    for r in rows:
+        if abs(r["cellMm"] - cell_mm) < 1e-9:
+            return {"discharged_ml": r["dischargedMl"], "shares": r["dischargedFractions"],
+                    "simulated_s": r.get("simulatedSeconds"), "wall_s_reference_laptop": r.get("wallSeconds")}
+    return None
+
+
+def run_whole_pour(args, precond: str) -> dict:
+    """The reference's own benchmark loop (benchmarks/run3d.ts:14-23): advance in 0.5 s chunks until 1.5 s
+    after the controller is done, through the public pl_advance call, timed by the host clock (end to end)
+    and by CUDA events on the engine's stream; then the same pour again with stage events, one substep per
+    launch, for the per-stage device time. No L2 flush: this is the continuous run the reference times."""
+    import torch
+
+    import teapotfluidsimulation_b200 as pkg
+
+    a = argparse.Namespace(**vars(args))
+    a.precond = precond
+
+    def make():
+        cfg = make_cfg(a)
+        cfg.device = torch.cuda.current_device()
+        return pkg.Simulation3D(cfg)
+
+    sim = make()
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    done_at = -1.0
+    while not sim.finished:
+        d = sim.advance(0.5)
+        if d["phase"] == "done" and done_at < 0:
+            done_at = d["time"]
+        if done_at >= 0 and d["time"] > done_at + 1.5:
+            break
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    dev_s = e0.elapsed_time(e1) / 1e3
+    d = sim.diagnostics()
+    sh = sim.discharged_fractions()
+    sim_s, substeps = d["time"], d["steps"]
+    sim.destroy()
+    out = {"simulated_s": sim_s, "substeps": substeps, "wall_s": wall, "sim_s_per_wall_s": sim_s / wall,
+           "device_s": dev_s, "sim_s_per_device_s": sim_s / dev_s,
+           "discharged_ml": d["dischargedMl"], "shares": None if sh is None else [float(v) for v in sh],
+           "spilled_ml": d["spilledMl"], "lost_ml": d["lostMl"], "pressure_failures": d["pressureFailures"]}
+    ref = reference_pour_result(args.cell_mm)
+    if ref is not None:
+        out["reference"] = ref
+        out["volume_rel_err"] = d["dischargedMl"] / ref["discharged_ml"] - 1
+        if sh is not None:
+            out["shares_max_abs_err"] = float(np.abs(np.array(sh) - np.array(ref["shares"])).max())
+    # the stage split of the same pour (one substep per launch, stage events in the graph)
+    sim = make()
+    sim.enable_stage_timing(True)
+    acc, its, cits, n = {}, [], [], 0
+    done_at = -1.0
+    while not sim.finished:
+        sim.enqueue(1)
+        sim.sync()
+        for k, v in sim.stage_times().items():
+            acc[k] = acc.get(k, 0.0) + v
+        dd = sim.diagnostics()
+        its.append(dd["pressureIterations"])
+        cits.append(dd["correctionIterations"])
+        n += 1
+        if dd["phase"] == "done" and done_at < 0:
+            done_at = dd["time"]
+        if done_at >= 0 and dd["time"] > done_at + 1.5:
+            break
+    sim.destroy()
+    out["stages_ms_per_substep"] = {k: v / max(n, 1) for k, v in acc.items()}
+    out["pressure_ms_per_substep"] = acc.get("pressure", 0.0) / max(n, 1)
+    out["correction_ms_per_substep"] = acc.get("correction", 0.0) / max(n, 1)
+    out["pressure_iterations_mean"] = float(np.mean(its)) if its else 0.0
+    out["correction_iterations_mean"] = float(np.mean(cits)) if cits else 0.0
+    out["pressure_iterations_max"] = int(max(its)) if its else 0
+    return out
 
 
 def run_reference(args):
@@ -563,42 +701,40 @@ def run_reference(args):
 
 
 def run_ours(args):
-    import ctypes
-
     import torch
 
     world, rank, local = dist_init()
     import teapotfluidsimulation_b200 as pkg
-    from teapotfluidsimulation_b200 import abi
 
     torch.cuda.set_device(local)
     cfg = make_cfg(args)
     cfg.device = local
-    sim = pkg.Simulation3D(cfg)
-    if args.start > 0:
-        sim.advance(args.start)
-    sim.enable_stage_timing(True)
-    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
 
-    def substep(stage_acc):
+    def started():
+        sim = pkg.Simulation3D(cfg)
+        if args.start > 0:
+            sim.advance(args.start)
+        return sim, torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+
+    # value: the production substep graph (no stage events), one graph launch per substep bracketed by CUDA
+    # events on the engine's stream, the L2 flushed before each substep outside the bracket
+    sim, stream = started()
+    start_state = (sim.get_state(), sim.particles())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def substep() -> float:
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
+        e0.record(stream)
         sim.enqueue(1)
+        e1.record(stream)
         sim.sync()
-        st = sim.stage_times()
-        if stage_acc is not None:
-            for k, v in st.items():
-                stage_acc[k] = stage_acc.get(k, 0.0) + v
-        return sum(st.values())
+        return e0.elapsed_time(e1)
 
     for _ in range(args.warmup):
-        substep(None)
+        substep()
     d0 = sim.diagnostics()
-    stage_acc: dict = {}
-    pcg_work = 0.0
-    iters = []
-    corr_iters = []
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -608,60 +744,88 @@ def run_ours(args):
     for _ in range(args.steps):
         if sim.finished:
             break
-        dev_ms += substep(stage_acc)
+        dev_ms += substep()
         steps_done += 1
-        d = sim.diagnostics()
+    torch.cuda.synchronize()
+    barrier(world)
+    d1 = sim.diagnostics()
+    sim_s = d1["time"] - d0["time"]
+    max_ms = allmax(dev_ms, world)
+    value = allsum(sim_s, world) / (max_ms / 1000.0)
+    sim.destroy()
+
+    # stage split of the same window: a second replica from the same start with stage events in its graph
+    ssim, sstream = started()
+    ssim.enable_stage_timing(True)
+    for _ in range(args.warmup):
+        with torch.cuda.stream(sstream):
+            flush.fill_(1.0)
+        ssim.enqueue(1)
+        ssim.sync()
+    stage_acc: dict = {}
+    pcg_work, iters, corr_iters = 0.0, [], []
+    for _ in range(steps_done):
+        with torch.cuda.stream(sstream):
+            flush.fill_(1.0)
+        ssim.enqueue(1)
+        ssim.sync()
+        for k, v in ssim.stage_times().items():
+            stage_acc[k] = stage_acc.get(k, 0.0) + v
+        d = ssim.diagnostics()
         iters.append(d["pressureIterations"])
         corr_iters.append(d["correctionIterations"])
         # the Chebyshev launch solves both systems (on two clusters at once): count both
         solved = d["pressureIterations"] + (d["correctionIterations"] if args.precond == "cheb" else 0)
         pcg_work += pcg_bytes_per_iteration(d["liquidCells"], args.precond, args.precision) * solved
-    torch.cuda.synchronize()
-    barrier(world)
-    clk = clocks.stop()
-    d1 = sim.diagnostics()
-    sim_s = d1["time"] - d0["time"]
-    max_ms = allmax(dev_ms, world)
-    total_sim = allsum(sim_s, world)
-    value = total_sim / (max_ms / 1000.0)
+    ssim.destroy()
 
-    # end to end through the C ABI: pl_step per substep on a second replica from the same start
-    e2e_sim = pkg.Simulation3D(make_cfg(args) if world == 1 else cfg)
-    if args.start > 0:
-        e2e_sim.advance(args.start)
+    # end to end through the C ABI: pl_step per substep (control block in, stats block out) from the same start
+    e2e_sim, _ = started()
     for _ in range(args.warmup):
         e2e_sim.step(-1.0)
-    e0 = e2e_sim.diagnostics()["time"]
+    e2e_t0 = e2e_sim.diagnostics()["time"]
     wall = 0.0
     for _ in range(steps_done):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
+        flush.fill_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e2e_sim.step(-1.0)
         wall += time.perf_counter() - t0
-    e2e_s = e2e_sim.diagnostics()["time"] - e0
+    e2e_s = e2e_sim.diagnostics()["time"] - e2e_t0
     e2e_value = allsum(e2e_s, world) / allmax(wall, world)
     scalars = int(e2e_sim.sizes.step_copy_bytes)  # the device scalar block, copied each way per pl_step
+    e2e_sim.destroy()
+
+    whole = None
+    if args.whole_pour:
+        whole = {"workload": f"the whole gentle pour at {args.cell_mm:g} mm from t = 0 until 1.5 s after the "
+                             f"controller is done (benchmarks/run3d.ts), pl_advance in 0.5 s chunks, no L2 flush"}
+        for pre in ("cheb", "mg"):
+            whole[pre] = run_whole_pour(args, pre)
+    clk = clocks.stop()
 
     peaks, peak_kind = measured_peaks()
-    pres_ms = stage_acc.get("pressure", 0.0) / max(steps_done, 1)
-    achieved = (pcg_work / max(steps_done, 1)) / (pres_ms / 1000.0) / 1e9 if pres_ms > 0 else 0.0
+    n = max(steps_done, 1)
+    pres_ms = stage_acc.get("pressure", 0.0) / n
+    achieved = (pcg_work / n) / (pres_ms / 1000.0) / 1e9 if pres_ms > 0 else 0.0
     traffic = profile_traffic()
     line = {
         "metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s", "n_gpus": world, "steps": steps_done,
-        "warmup": args.warmup, "ms_per_step": max_ms / max(steps_done, 1), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": max_ms / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": ("f32 solve vectors, f64 inner products/refinement" if args.precision == "mixed" else "f64 solve")
                  + " / f32 parcels and faces, f64 transfer weights", "data": "synthetic",
         "config": {"workload": WORKLOAD, "cell_mm": args.cell_mm, "preconditioner": args.precond,
                    "solve_shape": f"{cfg.solve_cluster}x{cfg.solve_threads}",
                    "solve_precision": args.precision,
                    "start_s": args.start, "simulated_s": sim_s, "l2": "256 MiB buffer written between substeps",
+                   "timing": "CUDA events around each substep graph launch (no stage events in the graph)",
                    "parallelism": f"replicas x{world}"},
         "pressure_ms_per_substep": pres_ms,
         "pressure_iterations_mean": (sum(iters) / len(iters)) if iters else 0,
         "correction_iterations_mean": (sum(corr_iters) / len(corr_iters)) if corr_iters else 0,
-        "stages_ms_per_substep": {k: v / max(steps_done, 1) for k, v in stage_acc.items()},
+        "stages_ms_per_substep": {k: v / n for k, v in stage_acc.items()},
+        "stages_note": "a separate replica from the same start with stage events in its graph; density runs "
+                       "beside P2G on a second stream (its time overlaps P2G's)",
         "gpu_launches": KERNELS_PER_SUBSTEP[args.precond] * steps_done,
         "e2e": {"value": e2e_value, "unit": "sim-s/wall-s", "h2d_bytes_per_step": scalars,
                 "d2h_bytes_per_step": scalars},
@@ -673,10 +837,12 @@ def run_ours(args):
                      "frac": achieved / peaks.get("hbm_gbs", 1.0), "peak_kind": peak_kind,
                      "traffic": traffic},
     }
+    if whole is not None:
+        line["whole_pour"] = whole
     if clk:
         line["clocks"] = clk
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        line["cpu_baseline"] = run_cpu_baseline(args, args.cpu_sample)
+        line["cpu_baseline"] = run_cpu_baseline(args, args.cpu_sample, start_state)
     pois = run_poisson(args, world, rank)
     if pois is not None:
         line["poisson_batch"] = pois
@@ -688,8 +854,6 @@ def run_ours(args):
         line["ensemble"] = ens
     if rank == 0:
         print(json.dumps(line))
-    e2e_sim.destroy()
-    sim.destroy()
     if world > 1:
         import torch.distributed as dist
 
