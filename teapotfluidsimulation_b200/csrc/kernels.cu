@@ -823,6 +823,9 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
   int meta = __float_as_int(vel.w);
   int st = meta & 0xff;
   const double dt = sc->dt;
+  if (st != IN_POT && g.apic)  // a removed parcel keeps its own affine state (the slot is re-used every substep)
+#pragma unroll
+    for (int a = 0; a < 3; a++) P.aff_home[a * g.n + p] = P.aff_sorted[a * g.n + p];
   if (st == DISCHARGED || st == SPILLED) {  // solver3d.ts:693-702
     if ((double)pos.y > -1) {
       double vy = (double)vel.y - g.gravity * dt;

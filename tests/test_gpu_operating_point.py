@@ -10,13 +10,17 @@ Tolerances:
   - cell types: bit-exact;
   - pressure and projected velocity after one substep, against the oracle solved to a max-norm
     relative residual of 1e-12 (the FP64 reference solution): relative L2 < 1e-5. The reference's
-    own MIC(0) solve at 1e-6 sits ~1e-7 from that solution at a 4 mm mid-pour state, so the bound
-    leaves a factor of ~100 for the engine's different preconditioner and FP32 vectors;
+    own MIC(0) solve at 1e-6 sits ~5e-8 from that solution at a 4 mm mid-pour state; measured for the
+    engine: Chebyshev/MIXED 1.3e-7 (velocity 2.1e-7), box multigrid 2.9e-7, cluster multigrid 4.9e-7,
+    MIC(0) 4.8e-8, and 3.2e-7 for the 2.5 mm full-domain APIC configuration;
   - particle-to-grid velocity (no solve involved): relative L2 < 1e-5;
   - density-correction velocity: both sides solve it to the reference's fixed 1e-4 tolerance with
-    different preconditioners, so it is compared at relative L2 < 2e-3;
-  - 200 substeps with the engine's own dt: simulated time and tilt angle within 2e-6 relative, MIC(0)
-    iteration count equal, max divergence within 5% and interior density within 1e-6.
+    different preconditioners, so it is compared at relative L2 < 2e-3 (measured 2e-4 to 3.4e-4);
+  - 200 substeps with the engine's own dt: with MIC(0), the reference's preconditioner, simulated time
+    and tilt angle within 2e-6 relative (measured 1.7e-7 and 7.2e-7), the iteration count equal, max
+    divergence within 5% (measured 3e-5) and interior density within 1e-6 (measured 3e-8). The
+    Chebyshev solve stops at a different iterate inside the same 1e-6 rule, which moves the velocities
+    and so every later stable dt by ~1e-6: time and angle within 1e-5 (measured 8e-7 and 3.6e-6).
 """
 import numpy as np
 import pytest
@@ -105,8 +109,9 @@ def test_200_substeps_with_the_engines_own_dt(engine, goldens, name):
           f"iters={d['pressureIterations']} (golden {g['pressureIterations']}) maxDiv={d['maxDivergence']!r} "
           f"(golden {g['maxDivergence']!r}) interior={d['interiorDensity']!r} (golden {g['interiorDensity']!r})")
     assert d["steps"] == 200
-    assert abs(d["time"] / g["time"] - 1) < 2e-6
-    assert abs(d["angleDeg"] / g["angleDeg"] - 1) < 2e-6
+    bound = 2e-6 if name == "mic0_f64" else 1e-5
+    assert abs(d["time"] / g["time"] - 1) < bound
+    assert abs(d["angleDeg"] / g["angleDeg"] - 1) < bound
     assert abs(d["interiorDensity"] - g["interiorDensity"]) < 1e-6
     assert abs(d["inPotMl"] - 1500) < 1e-6 and d["pressureFailures"] == 0
     if name == "mic0_f64":  # the reference's own preconditioner: the same iteration count
