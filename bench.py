@@ -741,12 +741,14 @@ def run_ours(args):
     clocks.start()
     dev_ms = 0.0
     steps_done = 0
+    torch.cuda.cudart().cudaProfilerStart()  # the timed window alone, for `ncu --profile-from-start off`
     for _ in range(args.steps):
         if sim.finished:
             break
         dev_ms += substep()
         steps_done += 1
     torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
     barrier(world)
     d1 = sim.diagnostics()
     sim_s = d1["time"] - d0["time"]
