@@ -20,7 +20,8 @@ Tolerances:
     and tilt angle within 2e-6 relative (measured 1.7e-7 and 7.2e-7), the iteration count equal, max
     divergence within 5% (measured 3e-5) and interior density within 1e-6 (measured 3e-8). The
     Chebyshev solve stops at a different iterate inside the same 1e-6 rule, which moves the velocities
-    and so every later stable dt by ~1e-6: time and angle within 1e-5 (measured 8e-7 and 3.6e-6).
+    and so every later stable dt by ~1e-6: time and angle within 1e-5 (measured 8e-7 and 3.6e-6),
+    interior density within 5e-6 (measured 1.3e-6).
 """
 import numpy as np
 import pytest
@@ -112,7 +113,7 @@ def test_200_substeps_with_the_engines_own_dt(engine, goldens, name):
     bound = 2e-6 if name == "mic0_f64" else 1e-5
     assert abs(d["time"] / g["time"] - 1) < bound
     assert abs(d["angleDeg"] / g["angleDeg"] - 1) < bound
-    assert abs(d["interiorDensity"] - g["interiorDensity"]) < 1e-6
+    assert abs(d["interiorDensity"] - g["interiorDensity"]) < (1e-6 if name == "mic0_f64" else 5e-6)
     assert abs(d["inPotMl"] - 1500) < 1e-6 and d["pressureFailures"] == 0
     if name == "mic0_f64":  # the reference's own preconditioner: the same iteration count
         assert d["pressureIterations"] == g["pressureIterations"]
