@@ -10,7 +10,9 @@ constexpr int CHEB_CLUSTER = 16;       // largest cluster (non-portable size, on
 constexpr int CHEB_MAX_THREADS = 1024;  // largest CTA
 constexpr int CHEB_SMEM = 220 * 1024;   // dynamic shared memory per CTA
 constexpr int CHEB_DEGREE = 12;        // polynomial degree (stencil applications per CG iteration)
-constexpr double CHEB_LO = 0.03;        // lower end of the D^-1 A interval the polynomial targets
+constexpr double CHEB_LO = 0.01;        // lower end of the D^-1 A interval the polynomial targets (the
+                                        // spectrum starts near 1e-3 on 4 mm pour systems; 0.01 takes
+                                        // ~10% fewer CG iterations than 0.03 at degree 12)
 constexpr int CHEB_KMAX = 4;           // most cells per thread (their state stays in registers)
 
 struct ChebArgs {
