@@ -108,22 +108,16 @@ __device__ __forceinline__ void st_async(uint32_t raddr, double v, uint32_t rbar
                : "memory");
 }
 
-// Shared-memory accesses by 32-bit address (volatile: they keep their order against the barrier waits).
-__device__ __forceinline__ double lds(uint32_t a, double) {
-  double v;
-  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
-  return v;
+// Plain shared-memory accesses at a byte offset into the dynamic shared memory. The round barriers
+// (__syncthreads, and the mbarrier waits whose asm clobbers memory) keep them in place, and the
+// compiler is free to issue a cell's six neighbour loads, and both cells' loads, back to back.
+template <typename V>
+__device__ __forceinline__ V ldsh(const char* smem, uint32_t off) {
+  return *reinterpret_cast<const V*>(smem + off);
 }
-__device__ __forceinline__ float lds(uint32_t a, float) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
-  return v;
-}
-__device__ __forceinline__ void sts(uint32_t a, double v) {
-  asm volatile("st.shared.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
-}
-__device__ __forceinline__ void sts(uint32_t a, float v) {
-  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+template <typename V>
+__device__ __forceinline__ void stsh(char* smem, uint32_t off, V v) {
+  *reinterpret_cast<V*>(smem + off) = v;
 }
 
 struct Cl {
@@ -137,8 +131,11 @@ struct Cl {
   double wpart[2][CHEB_MAX_THREADS / 32][3];
   double bcast[2][3];
   double coef[CHEB_MAX_DEGREE][2];  // Chebyshev step coefficients (c1, c2)
+  float coef_f[CHEB_MAX_DEGREE][2];  // ... rounded to FP32 once (the FP32-vector solve's step arithmetic)
   int out_cnt[CHEB_CLUSTER];  // distinct remote cells this rank references in each owner
   int in_cnt[CHEB_CLUSTER];   // requests each rank sends to this rank
+  int req_off[CHEB_CLUSTER];  // start of each rank's requests in this rank's request table
+  int hmin[CHEB_CLUSTER];     // first halo slot of each requesting rank's requests (its slots are consecutive)
   int out_pos[CHEB_CLUSTER];  // running position of this rank's requests in each owner's table
   int nh;                     // halo slots of this rank
 };
@@ -220,7 +217,7 @@ __device__ __forceinline__ V& sv(char* smem, uint32_t off, int i) {
 // K: cells per thread (1, 2 or 4; at most 1024 / K threads, so that the per-cell state stays in
 // registers).
 template <typename T, int K>
-__global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs P, SolverWs W, ChebArgs a) {
+__global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevPtrs P, SolverWs W, ChebArgs a) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
   if (a.gate && sc->mg_status) return;  // the launch before this one solved the system
@@ -283,6 +280,8 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       const double rhoN = 1 / (2 * sigma1 - rho);
       C.coef[s][0] = rhoN * rho;
       C.coef[s][1] = 2 * rhoN / delta;
+      C.coef_f[s][0] = float(C.coef[s][0]);
+      C.coef_f[s][1] = float(C.coef[s][1]);
       rho = rhoN;
     }
   }
@@ -375,9 +374,8 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   const uint32_t DV0 = take(size_t(n1) * sizeof(T)), DV1 = take(size_t(n1) * sizeof(T));
   const uint32_t ZS = take(size_t(n1) * sizeof(T));
   const uint32_t QS = take(size_t(n1) * 8);
-  const uint32_t DCNT = take(size_t(chunk) * 4);
-  const uint32_t DST = take(size_t(chunk) * 6 * 4);  // up to 6 requesting ranks per own cell
   const uint32_t REQ = take(size_t(chunk) * 6 * 8);  // (own local index, rank << 16 | slot)
+  const uint32_t SENDL = take(size_t(chunk) * 6 * 8);  // the same requests ordered by (rank, slot)
   if (off > BM || n1 > 65535) {  // uniform decision: the wavefront solver takes over
     if (me == 0 && tid == 0) sc->mg_status = 0;
     cl.sync();
@@ -394,7 +392,6 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     sv<T>(smem, DV0, i) = sv<T>(smem, DV1, i) = sv<T>(smem, ZS, i) = T(0);
     sv<double>(smem, QS, i) = 0;
   }
-  for (int i = tid; i < chunk; i += nt) sv<int>(smem, DCNT, i) = 0;
   __syncthreads();
   // ---- one request per referenced remote position, into its owner's table
   for (int w = tid; w < nwords; w += nt) {
@@ -425,19 +422,35 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       nbo[k][f] = uint32_t(li) * uint32_t(sizeof(T));
     }
   }
+  if (tid < ns) C.hmin[tid] = 0x7fffffff;
   cl.sync();  // every request is in its owner's table; no generic remote access after this
+  // Send list: every rank's requests sit in one block of the table (lower ranks first) in arbitrary
+  // order; its slots are the consecutive halo slots hmin .. hmin + count - 1 of that rank, so each
+  // request goes to block offset + (slot - hmin). Each round's send pass walks this list, so
+  // consecutive threads store to consecutive halo slots of one rank (coalesced remote stores:
+  // stores scattered over ranks and slots cost several times more on the cluster network).
   for (int i = tid; i < incoming; i += nt) {
     const uint2 rq = sv<uint2>(smem, REQ, i);
-    const int p = atomicAdd(&sv<int>(smem, DCNT, int(rq.x)), 1);
-    sv<uint32_t>(smem, DST, p * chunk + int(rq.x)) = rq.y;
+    atomicMin(&C.hmin[rq.y >> 16], int(rq.y & 0xffffu));
+  }
+  if (tid == 0) {
+    int o = 0;
+    for (int r = 0; r < ns; r++) {
+      C.req_off[r] = o;
+      o += C.in_cnt[r];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < incoming; i += nt) {
+    const uint2 rq = sv<uint2>(smem, REQ, i);
+    const int rk = int(rq.y >> 16), h = int(rq.y & 0xffffu);
+    sv<uint2>(smem, SENDL, C.req_off[rk] + h - C.hmin[rk]) = make_uint2(rq.x | (uint32_t(rk) << 16), uint32_t(h));
   }
   __syncthreads();
   // ---- per-thread state of the owned cells (the exchange data serves every job of the launch)
   T r[K], z[K], res[K], as[K], sown[K], cdown[K], idg[K], dg[K], w[K];
   double q[K], b64[K];
-  int li_own[K];            // liquid-list index of each own cell
-  int nd[K];                // requesting ranks
-  uint32_t d0a[K], d0b[K];  // the first one's halo slot (in its vector at offset 0) and exchange barrier
+  int li_own[K];  // liquid-list index of each own cell
 #pragma unroll
   for (int k = 0; k < K; k++) {
     const int t = tid + k * nt;
@@ -446,51 +459,32 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
     const double d = has[k] ? W.adiag[li] : 1.0;
     dg[k] = T(d);
     idg[k] = T(1) / T(d);
-    nd[k] = has[k] ? sv<int>(smem, DCNT, t) : 0;
-    d0a[k] = d0b[k] = 0;
-    if (nd[k] > 0) {
-      const uint32_t dd = sv<uint32_t>(smem, DST, t);
-      const int rk = int(dd >> 16);
-      d0a[k] = C.rsmem[rk] + uint32_t(guard + 1 + int(dd & 0xffffu)) * uint32_t(sizeof(T));
-      d0b[k] = C.rxbar[rk];
-    }
   }
-  const uint32_t sbase = s_addr(smem);
   const uint32_t xb0 = s_addr(&C.xbar[0]);
-  // Store v (a T) as own cell t_k of the vector at byte offset voff and into the halo slots of the
-  // requesting ranks, on this round's barrier.
+  // Store v (a T) as own cell t_k of the vector at byte offset voff (the round's send pass carries
+  // it to the requesting ranks).
   auto put = [&](uint32_t voff, int k, T v) {
-    const int t = tid + k * nt;
-    sts(sbase + voff + uint32_t(t) * uint32_t(sizeof(T)), v);
-    if (nd[k] > 0) {
-      const uint32_t bo = uint32_t(e & 1) * 8u;
-      st_async(d0a[k] + voff, v, d0b[k] + bo);
-      for (int j = 1; j < nd[k]; j++) {
-        const uint32_t dd = sv<uint32_t>(smem, DST, j * chunk + t);
-        const int rk = int(dd >> 16);
-        st_async(C.rsmem[rk] + voff + uint32_t(guard + 1 + int(dd & 0xffffu)) * uint32_t(sizeof(T)), v,
-                 C.rxbar[rk] + bo);
-      }
-    }
+    stsh<T>(smem, voff + uint32_t(tid + k * nt) * uint32_t(sizeof(T)), v);
   };
   // The same for an FP64 vector (the solution q in the FP32 refinement).
-  auto put64 = [&](uint32_t voff, int k, double v) {
-    const int t = tid + k * nt;
-    sts(sbase + voff + uint32_t(t) * 8u, v);
+  auto put64 = [&](uint32_t voff, int k, double v) { stsh<double>(smem, voff + uint32_t(tid + k * nt) * 8u, v); };
+  // End of an exchange round of the vector at byte offset voff, values of V: once every own value of
+  // the round is stored, the send pass stores each requested value into its halo slot of the
+  // requesting rank on that rank's barrier of this round; then warp 0 alone polls this rank's barrier
+  // (every halo slot received) and the CTA barrier after it orders every thread's reads of the round's
+  // own and received values after both (cheaper than 16 warps polling).
+  auto round_end = [&](uint32_t voff, auto vtype) {
+    using V = decltype(vtype);
+    __syncthreads();
     const uint32_t bo = uint32_t(e & 1) * 8u;
-    for (int j = 0; j < nd[k]; j++) {
-      const uint32_t dd = sv<uint32_t>(smem, DST, j * chunk + t);
-      const int rk = int(dd >> 16);
-      st_async(C.rsmem[rk] + voff + uint32_t(guard + 1 + int(dd & 0xffffu)) * 8u, v, C.rxbar[rk] + bo);
+    for (int i = tid; i < incoming; i += nt) {
+      const uint2 en = sv<uint2>(smem, SENDL, i);
+      const int rk = int(en.x >> 16);
+      const V v = ldsh<V>(smem, voff + (en.x & 0xffffu) * uint32_t(sizeof(V)));
+      st_async(C.rsmem[rk] + voff + (uint32_t(guard + 1) + en.y) * uint32_t(sizeof(V)), v, C.rxbar[rk] + bo);
     }
-  };
-  // End of an exchange round of values of vbytes bytes: own values visible to the CTA, every halo
-  // slot received.
-  // Warp 0 alone polls the barrier; the CTA barrier after it then orders every thread's reads of the
-  // round's own values and received halo values after both (cheaper than 16 warps polling).
-  auto round_end = [&](uint32_t vbytes) {
-    const uint32_t bar = xb0 + uint32_t(e & 1) * 8u;
-    if (tid == 0) mbar_expect(bar, uint32_t(nh) * vbytes);
+    const uint32_t bar = xb0 + bo;
+    if (tid == 0) mbar_expect(bar, uint32_t(nh) * uint32_t(sizeof(V)));
     if (tid < 32) mbar_wait(bar, uint32_t(e >> 1) & 1u, ok);
     __syncthreads();
     e++;
@@ -498,9 +492,9 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
   // Sum of the six neighbour values of own cell k in the vector at byte offset voff (pairwise: three
   // dependent additions).
   auto nsum = [&](uint32_t voff, int k) -> T {
-    const uint32_t vb = sbase + voff;
-    const T x0 = lds(vb + nbo[k][0], T()), x1 = lds(vb + nbo[k][1], T()), x2 = lds(vb + nbo[k][2], T());
-    const T x3 = lds(vb + nbo[k][3], T()), x4 = lds(vb + nbo[k][4], T()), x5 = lds(vb + nbo[k][5], T());
+    const T x0 = ldsh<T>(smem, voff + nbo[k][0]), x1 = ldsh<T>(smem, voff + nbo[k][1]);
+    const T x2 = ldsh<T>(smem, voff + nbo[k][2]), x3 = ldsh<T>(smem, voff + nbo[k][3]);
+    const T x4 = ldsh<T>(smem, voff + nbo[k][4]), x5 = ldsh<T>(smem, voff + nbo[k][5]);
     return ((x0 + x1) + (x2 + x3)) + (x4 + x5);
   };
   const T itheta = T(2.0 / (2.0 + a.cheb_lo));
@@ -517,9 +511,10 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
       put(out, k, d);
     }
     uint32_t last = out;
-    round_end(sizeof(T));
+    round_end(out, T());
     for (int s = 1; s < deg; s++) {
-      const T c1 = T(C.coef[s][0]), c2 = T(C.coef[s][1]);
+      const T c1 = sizeof(T) == 4 ? T(C.coef_f[s][0]) : T(C.coef[s][0]);
+      const T c2 = sizeof(T) == 4 ? T(C.coef_f[s][1]) : T(C.coef[s][1]);
       T acc[K];
 #pragma unroll
       for (int k = 0; k < K; k++) acc[k] = has[k] ? nsum(last, k) : T(0);
@@ -536,7 +531,7 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
         put(out, k, final_step ? z[k] : d);
       }
       last = out;
-      round_end(sizeof(T));
+      round_end(out, T());
     }
   };
   // w = A z from the published z; partial z.r and z.w
@@ -643,18 +638,18 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K) k_chebpcg(Geo g, DevPtrs
 #pragma unroll
         for (int k = 0; k < K; k++)
           if (has[k]) put64(QS, k, q[k]);
-        round_end(8);
+        round_end(QS, 0.0);
         double tm = 0;
         T rt[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
           rt[k] = T(0);
           if (!has[k]) continue;
-          const uint32_t qb = sbase + QS;
           constexpr uint32_t sc8 = 8 / sizeof(T);  // FP64 offsets from the T offsets
-          const double acc = ((lds(qb + nbo[k][0] * sc8, 0.0) + lds(qb + nbo[k][1] * sc8, 0.0)) +
-                              (lds(qb + nbo[k][2] * sc8, 0.0) + lds(qb + nbo[k][3] * sc8, 0.0))) +
-                             (lds(qb + nbo[k][4] * sc8, 0.0) + lds(qb + nbo[k][5] * sc8, 0.0));
+          const double acc =
+              ((ldsh<double>(smem, QS + nbo[k][0] * sc8) + ldsh<double>(smem, QS + nbo[k][1] * sc8)) +
+               (ldsh<double>(smem, QS + nbo[k][2] * sc8) + ldsh<double>(smem, QS + nbo[k][3] * sc8))) +
+              (ldsh<double>(smem, QS + nbo[k][4] * sc8) + ldsh<double>(smem, QS + nbo[k][5] * sc8));
           const double rd = b64[k] - (double(dg[k]) * q[k] - acc);
           tm = dmax(tm, fabs(rd));
           rt[k] = T(rd);
