@@ -120,6 +120,9 @@ struct SimScalars {
   // globaltimer stamps (ns) of a two-system cluster solve: start, start of the correction system,
   // end (the host splits the solve stage's event time into pressure and correction with them)
   unsigned long long t_solve[3];
+  // bits of the pose whose cosine and sine c1, s1 hold (the next substep reuses them as c0, s0); a
+  // NaN pattern when the host has set the pose, so that they are formed anew
+  unsigned long long phi_trig_bits;
 };
 
 // ---------------------------------------------------------------- frames (solver3d.ts:232-260)
@@ -264,6 +267,7 @@ struct DevPtrs {
   // faces
   float *u, *uprev, *uext;
   uint8_t *valid, *vext;
+  double* uc;  // density-correction face velocity -grad qc of this substep (valid when sc->corr_any)
   // liquid-cell work (solver), indexed by position in the liquid list
   double* rhs;      // density-correction rhs
   double* density;  // particle density

@@ -47,6 +47,10 @@ int fail(int code, const char* fmt, ...) {
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// A NaN bit pattern no pose takes: SimScalars.phi_trig_bits when the pose's cosine and sine must be
+// formed anew (a new simulation, or a state set from the host).
+constexpr unsigned long long kPoseTrigUnset = 0x7ff8dead00000001ull;
+
 }  // namespace
 
 struct pl_sim {
@@ -313,7 +317,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       B * 4,  B * 4,                                   // cnt, start
       C,      C * 4,  C * 4,                           // cell, lidx, list
       C * 8,  C * 8,                                   // q, qc
-      F * 4,  F * 4,  F * 4, F, F,                     // u, uprev, uext, valid, vext
+      F * 4,  F * 4,  F * 4, F, F, F * 8,              // u, uprev, uext, valid, vext, uc
       C * 8,  C * 8,                                   // rhs, density
       DENSITY_BLOCKS * 8, DENSITY_BLOCKS * 4,          // interior partials
       SCAN_MAX_TILES * 8,                              // scan descriptors
@@ -372,6 +376,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.uext = (float*)take();
   P.valid = (uint8_t*)take();
   P.vext = (uint8_t*)take();
+  P.uc = (double*)take();
   P.rhs = (double*)take();
   P.density = (double*)take();
   P.interior_part = (double*)take();
@@ -427,6 +432,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
                                                         : PL_PHASE_WAIT;
   hs.counts[0] = g.n;
   hs.interior = 1;
+  hs.phi_trig_bits = kPoseTrigUnset;
   rc = push_scalars(s);
   if (!rc) {
     std::vector<double> zero;
@@ -925,6 +931,7 @@ int pl_set_state(pl_sim* s, const pl_sim_state* st, const double* x, const doubl
     h.time = st->time;
     h.steps = st->steps;
     h.phi = st->phi;
+    h.phi_trig_bits = kPoseTrigUnset;  // the pose's cosine and sine are formed anew
     h.omega = st->omega;
     h.last_iters = st->last_iterations;
     h.failures = st->failures;

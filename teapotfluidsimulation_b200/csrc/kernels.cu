@@ -17,8 +17,9 @@
 //                     (solver3d.ts:627-670): it depends only on the parcels and the cell types, so
 //                     it runs before the solves
 //   [pressure solve, correction solve]  solver.cu / cheb.cu (one cluster launch for both)
-//   k_grad_ext1       u -= grad q, the first extrapolation layer, max divergence after projection
-//                     (solver3d.ts:496-528, 565-605, 473-493)
+//   k_grad_ext1       u -= grad q, the first extrapolation layer, max divergence after projection,
+//                     the correction face velocity -grad qc (solver3d.ts:496-528, 565-605, 473-493,
+//                     674)
 //   k_ext2            second extrapolation layer
 //   k_advect          FLIP/PIC grid-to-particle update, RK2 advection with the correction
 //                     velocity, SDF collision, symmetry plane, discharge and spill accounting
@@ -35,32 +36,51 @@ namespace pl {
 
 // ---------------------------------------------------------------- controller
 
+// One thread. Every field is read once up front (independent loads, one L2 round trip) and the
+// controller runs on local copies. The pose at the start of this substep is the last substep's new
+// pose, whose cosine and sine that substep already formed: they are reused when the pose's bits are
+// the ones they were formed for (the host setting a state clears that), so only the new pose's two
+// transcendentals stay on this kernel's path.
 __global__ void k_controller(Geo g, DevPtrs P) {
   SimScalars* sc = P.sc;
-  bool forced = sc->force_step != 0;
-  bool finished = sc->time >= g.duration - 1e-9;  // solver3d.ts:264-266
-  bool active = forced || (sc->time < sc->end_time - 1e-12 && !finished);  // solver3d.ts:283
+  const int force_step = sc->force_step;
+  const double time = sc->time, end_time = sc->end_time, forced_dt = sc->forced_dt;
+  const unsigned long long msb = sc->max_speed_bits;
+  const double omega0 = sc->omega, phi = sc->phi, c1p = sc->c1, s1p = sc->s1;
+  const unsigned long long phi_trig = sc->phi_trig_bits;
+  const int ndis = sc->counts[DISCHARGED];
+  const long long steps = sc->steps;
+  const pl_motion motion = sc->motion;
+  DevController ctl = sc->ctl;
+  const bool forced = force_step != 0;
+  const bool finished = time >= g.duration - 1e-9;  // solver3d.ts:264-266
+  const bool active = forced || (time < end_time - 1e-12 && !finished);  // solver3d.ts:283
   sc->active = active ? 1 : 0;
   if (!active) return;
   // stableDt (solver3d.ts:268-278) from the max speed of the last advection
-  double m = __longlong_as_double((long long)sc->max_speed_bits);
-  double speed = sqrt(m) + sqrt(5 * g.h * g.gravity) + fabs(sc->omega) * g.R;
+  double m = __longlong_as_double((long long)msb);
+  double speed = sqrt(m) + sqrt(5 * g.h * g.gravity) + fabs(omega0) * g.R;
   double dt = dmin(g.max_substep, (g.cfl * g.h) / speed);
-  dt = dmin(dt, g.duration - sc->time);  // solver3d.ts:284
-  if (forced && sc->forced_dt > 0) dt = sc->forced_dt;
+  dt = dmin(dt, g.duration - time);  // solver3d.ts:284
+  if (forced && forced_dt > 0) dt = forced_dt;
+  // step(dt) (solver3d.ts:288-292)
+  double discharged = ndis * g.parcel_volume * g.vol_factor;
+  double tilt1 = ctl_advance(motion, ctl, time + dt, dt, discharged);
+  double phi1 = -tilt1;
+  const bool reuse = (unsigned long long)__double_as_longlong(phi) == phi_trig;
+  const double c0 = reuse ? c1p : cos(phi), s0 = reuse ? s1p : sin(phi);
+  const double c1 = cos(phi1), s1 = sin(phi1);
   sc->force_step = 0;
   sc->forced_dt = 0;
-  // step(dt) (solver3d.ts:288-292)
-  double discharged = sc->counts[DISCHARGED] * g.parcel_volume * g.vol_factor;
-  double tilt1 = ctl_advance(sc->motion, sc->ctl, sc->time + dt, dt, discharged);
-  double phi1 = -tilt1;
-  sc->omega = (phi1 - sc->phi) / dt;
+  sc->ctl = ctl;
+  sc->omega = (phi1 - phi) / dt;
   sc->dt = dt;
   sc->phi1 = phi1;
-  sc->c0 = cos(sc->phi);
-  sc->s0 = sin(sc->phi);
-  sc->c1 = cos(phi1);
-  sc->s1 = sin(phi1);
+  sc->c0 = c0;
+  sc->s0 = s0;
+  sc->c1 = c1;
+  sc->s1 = s1;
+  sc->phi_trig_bits = (unsigned long long)__double_as_longlong(phi1);
   // per-substep counters
   sc->max_speed_bits = 0;
   sc->max_div_bits = 0;
@@ -69,8 +89,8 @@ __global__ void k_controller(Geo g, DevPtrs P) {
   sc->scan_tile = 0;
   // commit the pose and clock (solver3d.ts:306-308); kernels of this substep read phi0 from c0/s0
   sc->phi = phi1;
-  sc->time += dt;
-  sc->steps += 1;
+  sc->time = time + dt;
+  sc->steps = steps + 1;
 }
 
 // ---------------------------------------------------------------- binning
@@ -149,20 +169,24 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
+  constexpr int NW = SCAN_THREADS / 32;
   __shared__ int s_tile;
-  __shared__ unsigned long long s_warp[SCAN_THREADS / 32];
+  __shared__ unsigned long long s_seg[SCAN_ITEMS * NW];  // segment totals, then their exclusive prefixes
+  __shared__ unsigned long long s_agg;
   __shared__ unsigned long long s_prefix;
   if (threadIdx.x == 0) s_tile = atomicAdd(&sc->scan_tile, 1);
   __syncthreads();
   const int tile = s_tile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int b0 = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-  unsigned long long val[SCAN_ITEMS];
+  // Striped ownership: item e of a thread is bin tile * SCAN_TILE + e * SCAN_THREADS + threadIdx.x, so
+  // every load and store of the bin and cell arrays is coalesced. A warp's 32 bins of one item are a
+  // segment of consecutive bins; segment (e, warp) precedes segment (e, warp + 1) and (e + 1, 0).
+  const int b0 = tile * SCAN_TILE + threadIdx.x;
+  unsigned long long val[SCAN_ITEMS], incl[SCAN_ITEMS];
   uint8_t typ[SCAN_ITEMS];
-  unsigned long long local = 0;
 #pragma unroll
   for (int e = 0; e < SCAN_ITEMS; e++) {
-    int b = b0 + e;
+    int b = b0 + e * SCAN_THREADS;
     unsigned long long v = 0;
     typ[e] = AIR;
     if (b < g.nbins) {
@@ -183,29 +207,34 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       }
     }
     val[e] = v;
-    local += v;
-  }
-  // block exclusive scan of the per-thread totals
-  unsigned long long x = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    unsigned long long w = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0ull;
+    // inclusive scan of the warp's segment
+    unsigned long long x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
+      unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    if (lane < SCAN_THREADS / 32) s_warp[lane] = w;  // inclusive per warp
+    incl[e] = x;
+    if (lane == 31) s_seg[e * NW + warp] = x;
   }
   __syncthreads();
-  unsigned long long thread_excl = x - local + (warp > 0 ? s_warp[warp - 1] : 0ull);
-  unsigned long long aggregate = s_warp[SCAN_THREADS / 32 - 1];
+  // exclusive scan of the SCAN_ITEMS * NW segment totals (two per lane of warp 0), in bin order
+  if (warp == 0) {
+    static_assert(SCAN_ITEMS * NW == 64, "two segments per lane");
+    const unsigned long long a0 = s_seg[2 * lane], a1 = s_seg[2 * lane + 1];
+    unsigned long long x = a0 + a1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const unsigned long long ex = x - a0 - a1;
+    s_seg[2 * lane] = ex;
+    s_seg[2 * lane + 1] = ex + a0;
+    if (lane == 31) s_agg = x;
+  }
+  __syncthreads();
+  const unsigned long long aggregate = s_agg;
   // decoupled look-back (bounded waits), one warp reading 32 predecessor descriptors at a time: the
   // exclusive prefix is the sum of the aggregates back to the nearest inclusive prefix
   if (warp == 0) {
@@ -252,10 +281,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
     }
   }
   __syncthreads();
-  unsigned long long run = s_prefix + thread_excl;
 #pragma unroll
   for (int e = 0; e < SCAN_ITEMS; e++) {
-    int b = b0 + e;
+    const int b = b0 + e * SCAN_THREADS;
+    const unsigned long long run = s_prefix + s_seg[e * NW + warp] + incl[e] - val[e];  // exclusive prefix
     if (b < g.nbins) {
       P.start[b] = (int)(run & 0xffffffffull);
       if (b < g.nc) {
@@ -271,7 +300,6 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
         if (b == g.nc - 1) sc->m = lpos + (typ[e] == FLUID ? 1 : 0);
       }
     }
-    run += val[e];
   }
 }
 
@@ -586,6 +614,9 @@ __global__ void k_grad_ext1(Geo g, DevPtrs P) {
     if (F.comp == 0 && F.i < g.nx && P.cell[F.i + g.nx * (F.j + g.ny * F.k)] == FLUID)
       bits = (unsigned long long)__double_as_longlong(projected_div(g, P, F.i, F.j, F.k));
     grad_ext1_face(g, P, f, F);
+    // the correction velocity of every face, once (applyGradient into zeroed uc, vc, wc:
+    // solver3d.ts:629-631, 674); advection samples it like the velocity field
+    if (g.kappa > 0 && sc->corr_any) P.uc[f] = grad_term(g, P, P.qc, F.comp, F.i, F.j, F.k);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -794,19 +825,13 @@ __device__ __forceinline__ float4 interp_gradient(const Geo& g, const float* fie
   return make_float4((float)gx, (float)gy, (float)gz, 0.f);
 }
 
-// Correction velocity uc at face corners: the gradient of the correction potential evaluated on
-// the fly (applyGradient into zeroed uc,vc,wc: solver3d.ts:629-631, 674).
+// sample() of the correction velocity (solver3d.ts:386-408 on uc, vc, wc), an FP64 face field.
 __device__ __forceinline__ double sample_corr(const Geo& g, const DevPtrs& P, int comp, double x, double y,
                                               double z) {
   Sten s = face_stencil(g, comp, x, y, z);
-  int sx = g.nx + (comp == 0), sy = g.ny + (comp == 1);
   double all = 0;
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    int local = corner(s, c) - comp_base(g, comp);
-    int i = local % sx, j = (local / sx) % sy, k = local / (sx * sy);
-    all += corner_w(s, c) * grad_term(g, P, P.qc, comp, i, j, k);
-  }
+  for (int c = 0; c < 8; c++) all += corner_w(s, c) * P.uc[corner(s, c)];
   return all;
 }
 
