@@ -134,9 +134,8 @@ struct Cl {
   float coef_f[CHEB_MAX_DEGREE][2];  // ... rounded to FP32 once (the FP32-vector solve's step arithmetic)
   int out_cnt[CHEB_CLUSTER];  // distinct remote cells this rank references in each owner
   int in_cnt[CHEB_CLUSTER];   // requests each rank sends to this rank
-  int req_off[CHEB_CLUSTER];  // start of each rank's requests in this rank's request table
-  int hmin[CHEB_CLUSTER];     // first halo slot of each requesting rank's requests (its slots are consecutive)
-  int out_pos[CHEB_CLUSTER];  // running position of this rank's requests in each owner's table
+  int in_base[CHEB_CLUSTER];  // each referencing rank's halo slot of the first of this rank's cells it references
+  int req_off[CHEB_CLUSTER];  // start of each referencing rank's entries in this rank's send list
   int nh;                     // halo slots of this rank
 };
 
@@ -291,7 +290,6 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
     C.rrbar[tid] = mapa_u32(s_addr(&C.rbar[0]), tid);
     C.rred[tid] = mapa_u32(s_addr(&C.red[0][0][0]), tid);
     C.out_cnt[tid] = 0;
-    C.out_pos[tid] = 0;
   }
   for (int w = tid; w < nwords; w += nt) sv<uint32_t>(smem, BM, w) = 0u;
   __syncthreads();
@@ -349,20 +347,36 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
     return sv<int>(smem, BMP, w) + __popc(sv<uint32_t>(smem, BM, w) & ((1u << (gi & 31)) - 1u));
   };
   if (tid < ns && tid != me) C.out_cnt[tid] = hrank(min((tid + 1) * chunk, m)) - hrank(min(tid * chunk, m));
+  // Each rank's cells that a rank R references are exactly its cells with a neighbour owned by R (the
+  // neighbour relation is symmetric), so every rank derives its own send list locally. R tells each
+  // owner how many of its cells R references and R's halo slot of the first of them (R's slots for one
+  // owner are consecutive and in position order).
   __syncthreads();
-  // tell every owner how many requests it gets from this rank
   if (tid < ns) {
     Cl* dst = cl.map_shared_rank(&C, tid);
     dst->in_cnt[me] = C.out_cnt[tid];
+    dst->in_base[me] = tid == me ? 0 : hrank(min(tid * chunk, m));
   }
-  cl.sync();  // in_cnt complete everywhere; barrier initialisation visible to the cluster
+  // destination ranks of every own cell (bit R: a neighbour is owned by R), counted per warp and rank
+  uint32_t dmask[K];
+  const int lane = tid & 31, wid = tid >> 5, nwarps = nt >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    uint32_t mk = 0;
+#pragma unroll
+    for (int f = 0; f < 6; f++) {
+      const int gi = gnb[k][f];
+      if (gi >= 0 && gi / chunk != me) mk |= 1u << (gi / chunk);
+    }
+    dmask[k] = mk;
+  }
+  cl.sync();  // in_cnt / in_base complete everywhere; barrier initialisation visible to the cluster
   const int nh = C.nh;
   int incoming = 0;
   for (int r = 0; r < ns; r++) incoming += C.in_cnt[r];
   int rr = 0;  // reduction counter (advances identically in every thread)
   int e = 0;   // exchange-round counter (likewise)
   bool ok = true;
-  const int hcap = int(reduce3(double(nh), 0.0, 0.0, C, rr, me, ns, ok).x);
   // ---- layout (identical in every rank): byte offsets into the dynamic shared memory
   uint32_t off = 0;
   auto take = [&](size_t bytes) -> uint32_t {
@@ -370,45 +384,68 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
     off += uint32_t((bytes + 15) & ~size_t(15));
     return r;
   };
+  const uint32_t WCNT = take(size_t(K) * CHEB_CLUSTER * (CHEB_MAX_THREADS / 32) * 4);  // per (k, rank, warp)
+  const uint32_t SENDL = take(size_t(chunk) * 6 * 8);  // (own index | rank << 16, halo slot), by (rank, slot)
+  const uint32_t VEC0 = off;
+  // per (k, rank, warp): cells of the warp's k-th group with a neighbour owned by the rank
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    for (int r = 0; r < ns; r++) {
+      const unsigned bal = __ballot_sync(0xffffffffu, (dmask[k] >> r) & 1u);
+      if (lane == 0) sv<int>(smem, WCNT, (k * CHEB_CLUSTER + r) * (CHEB_MAX_THREADS / 32) + wid) = __popc(bal);
+    }
+  __syncthreads();
+  // each rank's counts into exclusive offsets in (k, warp) order, i.e. in position order; a count that
+  // disagrees with what the rank expects (it cannot, the relation being symmetric) is flagged
+  double mismatch = 0;
+  if (tid < ns) {
+    int acc = 0;
+    for (int k = 0; k < K; k++)
+      for (int w = 0; w < nwarps; w++) {
+        int& c = sv<int>(smem, WCNT, (k * CHEB_CLUSTER + tid) * (CHEB_MAX_THREADS / 32) + w);
+        const int v = c;
+        c = acc;
+        acc += v;
+      }
+    if (tid != me && acc != C.in_cnt[tid]) mismatch = 1;
+    if (tid == me && acc != 0) mismatch = 1;
+    int o = 0;
+    for (int r = 0; r < tid; r++) o += C.in_cnt[r];
+    C.req_off[tid] = o;
+  }
+  // largest halo over the ranks (every rank's layout is the same) and the consistency flag, in one
+  // cluster-wide reduction
+  const double3 hm = reduce3(double(nh), mismatch, 0.0, C, rr, me, ns, ok);
+  const int hcap = int(hm.x);
   const int n1 = chunk + 1 + hcap;  // own cells, guard, halo
+  off = VEC0;
   const uint32_t DV0 = take(size_t(n1) * sizeof(T)), DV1 = take(size_t(n1) * sizeof(T));
   const uint32_t ZS = take(size_t(n1) * sizeof(T));
   const uint32_t QS = take(size_t(n1) * 8);
-  const uint32_t REQ = take(size_t(chunk) * 6 * 8);  // (own local index, rank << 16 | slot)
-  const uint32_t SENDL = take(size_t(chunk) * 6 * 8);  // the same requests ordered by (rank, slot)
-  if (off > BM || n1 > 65535) {  // uniform decision: the wavefront solver takes over
+  if (off > BM || n1 > 65535 || hm.y != 0) {  // uniform decision: the wavefront solver takes over
     if (me == 0 && tid == 0) sc->mg_status = 0;
     cl.sync();
     return;
-  }
-  // my requests' offset in each owner's table: the requests of lower ranks come first
-  if (tid < ns) {
-    const Cl* own = cl.map_shared_rank(&C, tid);
-    int o = 0;
-    for (int r = 0; r < me; r++) o += own->in_cnt[r];
-    C.out_pos[tid] = o;
   }
   for (int i = tid; i < n1; i += nt) {
     sv<T>(smem, DV0, i) = sv<T>(smem, DV1, i) = sv<T>(smem, ZS, i) = T(0);
     sv<double>(smem, QS, i) = 0;
   }
-  __syncthreads();
-  // ---- one request per referenced remote position, into its owner's table
-  for (int w = tid; w < nwords; w += nt) {
-    uint32_t bits = sv<uint32_t>(smem, BM, w);
-    int h = sv<int>(smem, BMP, w);
-    while (bits) {
-      const int b = __ffs(bits) - 1;
-      bits &= bits - 1u;
-      const int gi = (w << 5) + b;
-      const int rk = gi / chunk;
-      const int pos = atomicAdd(&C.out_pos[rk], 1);
-      char* owner = static_cast<char*>(cl.map_shared_rank(static_cast<void*>(smem), rk));
-      reinterpret_cast<uint2*>(owner + REQ)[pos] =
-          make_uint2(uint32_t(gi - rk * chunk), (uint32_t(me) << 16) | uint32_t(h));
-      h++;
+  // Send list, ordered by (rank, halo slot): each round's send pass walks it, so consecutive threads
+  // store to consecutive halo slots of one rank (coalesced remote stores: stores scattered over ranks
+  // and slots cost several times more on the cluster network).
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    for (int r = 0; r < ns; r++) {
+      const bool mine = (dmask[k] >> r) & 1u;
+      const unsigned bal = __ballot_sync(0xffffffffu, mine);
+      if (mine) {
+        const int idx = sv<int>(smem, WCNT, (k * CHEB_CLUSTER + r) * (CHEB_MAX_THREADS / 32) + wid) +
+                        __popc(bal & ((1u << lane) - 1u));
+        sv<uint2>(smem, SENDL, C.req_off[r] + idx) =
+            make_uint2(uint32_t(tid + k * nt) | (uint32_t(r) << 16), uint32_t(C.in_base[r] + idx));
+      }
     }
-  }
   // byte offsets of the own cells' neighbours in a stencil vector of T (the guard for none)
   uint32_t nbo[K][6];
   bool has[K];
@@ -421,30 +458,6 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
       const int li = gi < 0 ? guard : (gi / chunk == me ? gi - own0 : guard + 1 + hrank(gi));
       nbo[k][f] = uint32_t(li) * uint32_t(sizeof(T));
     }
-  }
-  if (tid < ns) C.hmin[tid] = 0x7fffffff;
-  cl.sync();  // every request is in its owner's table; no generic remote access after this
-  // Send list: every rank's requests sit in one block of the table (lower ranks first) in arbitrary
-  // order; its slots are the consecutive halo slots hmin .. hmin + count - 1 of that rank, so each
-  // request goes to block offset + (slot - hmin). Each round's send pass walks this list, so
-  // consecutive threads store to consecutive halo slots of one rank (coalesced remote stores:
-  // stores scattered over ranks and slots cost several times more on the cluster network).
-  for (int i = tid; i < incoming; i += nt) {
-    const uint2 rq = sv<uint2>(smem, REQ, i);
-    atomicMin(&C.hmin[rq.y >> 16], int(rq.y & 0xffffu));
-  }
-  if (tid == 0) {
-    int o = 0;
-    for (int r = 0; r < ns; r++) {
-      C.req_off[r] = o;
-      o += C.in_cnt[r];
-    }
-  }
-  __syncthreads();
-  for (int i = tid; i < incoming; i += nt) {
-    const uint2 rq = sv<uint2>(smem, REQ, i);
-    const int rk = int(rq.y >> 16), h = int(rq.y & 0xffffu);
-    sv<uint2>(smem, SENDL, C.req_off[rk] + h - C.hmin[rk]) = make_uint2(rq.x | (uint32_t(rk) << 16), uint32_t(h));
   }
   __syncthreads();
   // ---- per-thread state of the owned cells (the exchange data serves every job of the launch)
