@@ -119,3 +119,23 @@ def test_reused_solver_matches_a_fresh_one(trained, engine):
     it_b, x_b = run(pb, reduced, r[:2])
     pb.destroy()
     assert np.array_equal(it_a, it_b) and np.array_equal(x_a, x_b)
+
+
+def test_learned_cg_against_multigrid_pcg_in_wall_time(trained, engine):
+    # What the trained network gains over the method without it, in device time: flexible CG with the
+    # network against multigrid PCG, the same held-out systems, the same max-norm 1e-6 rule, the fastest
+    # of three solves each. The north star asks for at most 0.5x; measured at these 64x64x16 boxes the
+    # learned solve takes more time than multigrid PCG although the network alone converges (fewer than
+    # 2x the iterations): one application of the network costs far more than one V-cycle. The bound
+    # below holds the measured state (about 20x) against regressions; the ratio is printed.
+    Lr, box, cells, r, e, net, hist = trained
+    E = engine.engine
+    ho = slice(TRAIN, None)
+    _, it_mg, conv_mg, ms_mg = Lr.solve(box, cells[ho], r[ho], E.POISSON_MG, reps=3)
+    _, it_ln, conv_ln, ms_ln = Lr.solve(box, cells[ho], r[ho], E.POISSON_LEARNED, net=net, reps=3)
+    ratio = ms_ln / ms_mg
+    print(f"\nlearned FCG {ms_ln:.2f} ms ({it_ln.mean():.1f} iterations) vs multigrid PCG {ms_mg:.2f} ms "
+          f"({it_mg.mean():.1f} iterations) on {cells[ho].shape[0]} held-out systems: {ratio:.1f}x")
+    assert conv_mg.all() and conv_ln.all()
+    assert it_ln.max() < 2 * it_mg.max() + 8  # the network preconditions nearly as well per iteration
+    assert 0 < ratio < 60
