@@ -48,6 +48,9 @@ constexpr int TILE_PLANES_MAX = 8192;
 struct Geo {
   int nx, ny, nz, n;
   int nc, nu, nv, nw, nf;
+  // 1 / sx and 1 / (sx * sy) of each face component's extents (sx = nx + (comp == 0), ...), for
+  // decode_face's quotients (geo_face_reciprocals fills them)
+  float inv_sx[3], inv_sxy[3];
   int nbins;
   double h;
   double pwx, pwy;    // pivotWorld
@@ -220,6 +223,25 @@ PL_HD double js_hypot2(double a, double b) {
 struct Face {
   int comp, i, j, k, sx, sy, sz, local;
 };
+// floor(n / d) for 0 <= n < 2^24 and 1 <= d with the quotient below 2^20, from the float reciprocal
+// inv = 1/d: the product's relative error is below 2^-22, so the truncated estimate is off by at most
+// one, which the exact integer remainder corrects.
+PL_HD int quot_small(int n, int d, float inv) {
+  int q = int(float(n) * inv);
+  const int r = n - q * d;
+  if (r < 0) q--;
+  else if (r >= d) q++;
+  return q;
+}
+
+PL_HD void geo_face_reciprocals(Geo& g) {
+  for (int c = 0; c < 3; c++) {
+    const int sx = g.nx + (c == 0), sy = g.ny + (c == 1);
+    g.inv_sx[c] = 1.0f / float(sx);
+    g.inv_sxy[c] = 1.0f / float(sx * sy);
+  }
+}
+
 PL_HD Face decode_face(const Geo& g, int f) {
   Face r;
   int rem = f;
@@ -236,9 +258,11 @@ PL_HD Face decode_face(const Geo& g, int f) {
   r.sy = g.ny + (r.comp == 1);
   r.sz = g.nz + (r.comp == 2);
   r.local = rem;
-  r.i = rem % r.sx;
-  r.j = (rem / r.sx) % r.sy;
-  r.k = rem / (r.sx * r.sy);
+  const int sxy = r.sx * r.sy;
+  r.k = quot_small(rem, sxy, g.inv_sxy[r.comp]);
+  const int in_plane = rem - r.k * sxy;
+  r.j = quot_small(in_plane, r.sx, g.inv_sx[r.comp]);
+  r.i = in_plane - r.j * r.sx;
   return r;
 }
 PL_HD int comp_base(const Geo& g, int comp) { return comp == 0 ? 0 : comp == 1 ? g.nu : g.nu + g.nv; }

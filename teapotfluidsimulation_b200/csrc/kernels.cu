@@ -377,10 +377,16 @@ __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int
 #pragma unroll
   for (int q = 0; q < 27; q++) sw[q] = swv[q] = 0.0;
   const int ci = c % g.nx, cj = (c / g.nx) % g.ny, ck = c / (g.nx * g.ny);
+  // the next parcel's fraction and velocity are loaded while this one is summed
+  float4 fr_next = P.frac_sorted[p0];
+  float v_next = COMP < 3 ? reinterpret_cast<const float*>(&P.vel_sorted[p0])[COMP] : 0.f;
   for (int p = p0; p < p1; p++) {
-    const float4 fr = P.frac_sorted[p];
-    double v = 0.0;
-    if (COMP < 3) v = (double)reinterpret_cast<const float*>(&P.vel_sorted[p])[COMP];
+    const float4 fr = fr_next;
+    const double v = (double)v_next;
+    if (p + 1 < p1) {
+      fr_next = P.frac_sorted[p + 1];
+      if (COMP < 3) v_next = reinterpret_cast<const float*>(&P.vel_sorted[p + 1])[COMP];
+    }
     double wx[3], wy[3], wz[3];
     axis_w3(fr.x, hx, wx);
     axis_w3(fr.y, hy, wy);
@@ -426,27 +432,21 @@ __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int
   }
 }
 
-// One thread per (occupied cell, component); blockIdx.y is the component (3 = density).
+// One thread per (occupied cell, component); blockIdx.y is the component (3 = density). One
+// instantiation per transfer, chosen on the host, so the FLIP/PIC kernel is not held to the APIC
+// kernel's register count.
+template <bool APIC>
 __global__ void k_p2g_cells(Geo g, DevPtrs P) {
   if (!P.sc->active) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= g.nc) return;
   const int p0 = P.start[c], p1 = P.start[c + 1];
   if (p0 == p1) return;
-  if (g.apic) {
-    switch (blockIdx.y) {
-      case 0: cell_moments<0, true>(g, P, c, p0, p1); break;
-      case 1: cell_moments<1, true>(g, P, c, p0, p1); break;
-      case 2: cell_moments<2, true>(g, P, c, p0, p1); break;
-      default: cell_moments<3, true>(g, P, c, p0, p1); break;
-    }
-  } else {
-    switch (blockIdx.y) {
-      case 0: cell_moments<0, false>(g, P, c, p0, p1); break;
-      case 1: cell_moments<1, false>(g, P, c, p0, p1); break;
-      case 2: cell_moments<2, false>(g, P, c, p0, p1); break;
-      default: cell_moments<3, false>(g, P, c, p0, p1); break;
-    }
+  switch (blockIdx.y) {
+    case 0: cell_moments<0, APIC>(g, P, c, p0, p1); break;
+    case 1: cell_moments<1, APIC>(g, P, c, p0, p1); break;
+    case 2: cell_moments<2, APIC>(g, P, c, p0, p1); break;
+    default: cell_moments<3, APIC>(g, P, c, p0, p1); break;
   }
 }
 
@@ -1057,14 +1057,20 @@ void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st) {
 }
 
 void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st) {
-  k_p2g_cells<<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+  if (g.apic)
+    k_p2g_cells<true><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+  else
+    k_p2g_cells<false><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
 }
 
 // The cells' node partials, then the faces (k_p2g, this stream) and the density stage (k_density,
 // the second stream) side by side: both only read the partials, and they write disjoint arrays.
 void launch_p2g_cells(const Geo& g, const DevPtrs& P, cudaStream_t st) {
-  k_p2g_cells<<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+  if (g.apic)
+    k_p2g_cells<true><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+  else
+    k_p2g_cells<false><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
 }
 void launch_p2g_faces(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);

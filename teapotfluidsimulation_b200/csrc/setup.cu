@@ -110,6 +110,7 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
   g.nv = g.nx * (g.ny + 1) * g.nz;
   g.nw = g.nx * g.ny * (g.nz + 1);
   g.nf = g.nu + g.nv + g.nw;
+  geo_face_reciprocals(g);
   g.nbins = g.nc + REMOVED_BINS;
   if (g.nbins > SCAN_MAX_BINS) {
     snprintf(err, errlen, "pl_create: %d cells exceed the bin scan capacity", g.nc);
@@ -192,6 +193,7 @@ int host_construct(const pl_config& cfg, HostInit* out, char* err, size_t errlen
     g.nv = g.nx * (g.ny + 1) * g.nz;
     g.nw = g.nx * g.ny * (g.nz + 1);
     g.nf = g.nu + g.nv + g.nw;
+  geo_face_reciprocals(g);
     g.nbins = g.nc + REMOVED_BINS;
     if (g.nbins > SCAN_MAX_BINS) {
       snprintf(err, errlen, "pl_create: %d cells exceed the bin scan capacity", g.nc);
