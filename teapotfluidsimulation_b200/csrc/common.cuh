@@ -112,7 +112,7 @@ struct SimScalars {
   int outliers;  // in-pot parcels outside the interior cells (clamped into it)
   int corr_any;  // density rhs has a non-zero entry
   int mg_status;  // 1: the cluster multigrid solve ran; 0: the wavefront solver must run
-  int pad2;
+  int n_occ_solid;  // SOLID cells holding in-pot parcels this substep (entries of DevPtrs::occ_solid)
   unsigned long long max_speed_bits;  // max |v|^2 (FP64 bits) of in-pot parcels after advect
   unsigned long long max_div_bits;    // max |div| (FP64 bits) after projection
   double interior;                    // mean interior density ratio
@@ -267,6 +267,17 @@ PL_HD Face decode_face(const Geo& g, int f) {
 }
 PL_HD int comp_base(const Geo& g, int comp) { return comp == 0 ? 0 : comp == 1 ? g.nu : g.nu + g.nv; }
 
+// Bricks of BRICK_W^3 cells: a coarse occupancy map lets the face pass skip the neighbourhood gathers
+// of faces that no parcel can reach.
+constexpr int BRICK_W = 4;
+PL_HD int brick_count(const Geo& g) {
+  return ((g.nx + BRICK_W - 1) / BRICK_W) * ((g.ny + BRICK_W - 1) / BRICK_W) * ((g.nz + BRICK_W - 1) / BRICK_W);
+}
+PL_HD int brick_of(const Geo& g, int i, int j, int k) {
+  const int bnx = (g.nx + BRICK_W - 1) / BRICK_W, bny = (g.ny + BRICK_W - 1) / BRICK_W;
+  return i / BRICK_W + bnx * (j / BRICK_W + bny * (k / BRICK_W));
+}
+
 // Cell type with the solid border outside the grid (solver3d.ts:453-469).
 __device__ __forceinline__ uint8_t cell_at(const Geo& g, const uint8_t* cell, int i, int j, int k) {
   if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) return SOLID;
@@ -312,6 +323,12 @@ struct DevPtrs {
   // at offset slot = (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1) from the cell; m_den[slot * nc + c] =
   // sum w for the cell-centred node at that offset (density)
   uint8_t* occ;  // cell holds in-pot parcels
+  // per 4 x 4 x 4 brick of cells (brick_of): some cell of the brick holds in-pot parcels (written by
+  // the cell-partials pass, read by the face pass)
+  uint8_t* brick_occ;
+  // the SOLID cells that hold in-pot parcels (n_occ_solid of them, in no fixed order); with the liquid
+  // list they are every occupied cell
+  int* occ_solid;
   float2* m_vel;
   float* m_den;
   // grid-scale solves: the liquid system embedded in the box (cell types, rhs), the box solution and

@@ -332,6 +332,7 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
       g.box_solve ? NB : 16, g.box_solve ? NB * 4 : 16,  // grid-scale solves: box cells, rhs
       g.box_solve ? NB * 8 : 16, 32,                     // box solution, outcome
       g.box_solve ? NB * 4 : 16, g.box_solve ? NB * 8 : 16, 32,  // the correction's rhs, solution, outcome
+      size_t(brick_count(g)), C * 4,                     // brick occupancy, occupied solid cells
   };
   size_t total = 0;
   for (size_t b : sizes) total += al256(b);
@@ -403,6 +404,8 @@ int pl_create(const pl_config* cfg, pl_sim** out) {
   P.box_b2 = (float*)take();
   P.box_x2 = (double*)take();
   P.box_out2 = (double*)take();
+  P.brick_occ = (uint8_t*)take();
+  P.occ_solid = (int*)take();
   if (g.box_solve) {
     int brc = 0;
     char berr[256] = "";

@@ -134,6 +134,8 @@ __global__ void k_bin_count(Geo g, DevPtrs P) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < SCAN_MAX_TILES) P.scan_state[s] = 0ull;
   if (g.tiled && s < g.ntx * g.nty * g.nz) P.tile_mask[s] = 0ull;
+  if (s < brick_count(g)) P.brick_occ[s] = 0;  // brick_count <= nc
+  if (s == 0) P.sc->n_occ_solid = 0;
   if (s < g.nc) P.cell[s] = solid_or_air(g, P.sc, s);
   if (s >= g.n) return;
   float4 p = P.pos_home[s];
@@ -196,6 +198,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_classify(Geo g, DevPtrs P
       if (b < g.nc) {
         const uint8_t base = P.cell[b];  // SOLID or AIR from k_bin_count (solver3d.ts:313-336)
         typ[e] = base == SOLID ? SOLID : cn > 0 ? FLUID : AIR;
+        if (cn > 0 && base == SOLID) P.occ_solid[atomicAdd(&sc->n_occ_solid, 1)] = b;
         if (typ[e] == FLUID) {
           v += 1ull << 32;
           if (g.tiled) {
@@ -341,6 +344,10 @@ __global__ void k_bin_permute(Geo g, DevPtrs P) {
 
 // ---------------------------------------------------------------- particle-to-grid
 
+// The cell-partials pass: 128-thread blocks, 148 per component, so that the four components' blocks
+// (four per SM at its register count) are resident at once and stride over the occupied cells.
+constexpr int P2G_CELL_THREADS = 128, P2G_CELL_BLOCKS = 148;
+
 // Weights along one axis of a parcel with FP64-derived cell fraction f for the nodes at offsets -1,
 // 0, +1 from its cell: on a face axis (offset 0) the nodes 0 and +1; on a cell-centred axis (offset
 // 1/2) the nodes (-1, 0) or (0, +1) by which half of the cell the parcel is in (solver3d.ts:352-360).
@@ -432,22 +439,54 @@ __device__ __forceinline__ void cell_moments(const Geo& g, const DevPtrs& P, int
   }
 }
 
-// One thread per (occupied cell, component); blockIdx.y is the component (3 = density). One
+// The face pass's brick map (cleared by k_bin_count): occupied cell c marks its own brick and, where
+// it lies on a brick face, the bricks across that face (edges and corners included), so that the brick
+// of every cell within one cell of c, per axis, is marked.
+__device__ __forceinline__ void mark_bricks(const Geo& g, const DevPtrs& P, int c) {
+  const int i = c % g.nx, j = (c / g.nx) % g.ny, k = c / (g.nx * g.ny);
+  const int bi = i / BRICK_W, bj = j / BRICK_W, bk = k / BRICK_W;
+  const int bnx = (g.nx + BRICK_W - 1) / BRICK_W, bny = (g.ny + BRICK_W - 1) / BRICK_W;
+  const int bnz = (g.nz + BRICK_W - 1) / BRICK_W;
+  auto lo = [](int x, int b) { return x % BRICK_W == 0 && b > 0 ? -1 : 0; };
+  auto hi = [](int x, int b, int nb) { return x % BRICK_W == BRICK_W - 1 && b + 1 < nb ? 1 : 0; };
+  const int i0 = lo(i, bi), i1 = hi(i, bi, bnx), j0 = lo(j, bj), j1 = hi(j, bj, bny);
+  const int k0 = lo(k, bk), k1 = hi(k, bk, bnz);
+  for (int dk = k0; dk <= k1; dk++)
+    for (int dj = j0; dj <= j1; dj++)
+      for (int di = i0; di <= i1; di++) P.brick_occ[(bi + di) + bnx * ((bj + dj) + bny * (bk + dk))] = 1;
+}
+
+// One thread per (occupied cell, component); blockIdx.y is the component (3 = density). The occupied
+// cells are the liquid list's (every non-solid cell with parcels) and the solid cells with parcels, so
+// the grid strides over that compact range (its size is known on the device only) instead of the whole
+// grid. Each cell's partials depend on that cell alone, so the order of the cells is free. One
 // instantiation per transfer, chosen on the host, so the FLIP/PIC kernel is not held to the APIC
 // kernel's register count.
 template <bool APIC>
-__global__ void k_p2g_cells(Geo g, DevPtrs P) {
-  if (!P.sc->active) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= g.nc) return;
-  const int p0 = P.start[c], p1 = P.start[c + 1];
-  if (p0 == p1) return;
-  switch (blockIdx.y) {
-    case 0: cell_moments<0, APIC>(g, P, c, p0, p1); break;
-    case 1: cell_moments<1, APIC>(g, P, c, p0, p1); break;
-    case 2: cell_moments<2, APIC>(g, P, c, p0, p1); break;
-    default: cell_moments<3, APIC>(g, P, c, p0, p1); break;
+__global__ void __launch_bounds__(P2G_CELL_THREADS) k_p2g_cells(Geo g, DevPtrs P) {
+  const SimScalars* sc = P.sc;
+  if (!sc->active) return;
+  const int m = sc->m, total = m + sc->n_occ_solid;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int c = t < m ? P.list[t] : P.occ_solid[t - m];
+    const int p0 = P.start[c], p1 = P.start[c + 1];
+    if (blockIdx.y == 0) mark_bricks(g, P, c);
+    switch (blockIdx.y) {
+      case 0: cell_moments<0, APIC>(g, P, c, p0, p1); break;
+      case 1: cell_moments<1, APIC>(g, P, c, p0, p1); break;
+      case 2: cell_moments<2, APIC>(g, P, c, p0, p1); break;
+      default: cell_moments<3, APIC>(g, P, c, p0, p1); break;
+    }
   }
+}
+
+// Whether a source cell of face (comp, i, j, k) in face_sums may hold parcels. The source cells are
+// within one cell of cell (i, j, k) per axis (offsets {-1, 0} on the face axis, {-1, 0, +1} on the
+// others), so one of them holding parcels marks the brick of (i, j, k) (mark_bricks); the last face
+// of an axis (i = nx, ...) reads the brick of the cell before it. A face that no parcel reaches sums
+// nothing: its weights and weighted velocities are 0.
+__device__ __forceinline__ bool face_reached(const Geo& g, const DevPtrs& P, int i, int j, int k) {
+  return P.brick_occ[brick_of(g, min(i, g.nx - 1), min(j, g.ny - 1), min(k, g.nz - 1))] != 0;
 }
 
 // Weighted sums at face (i, j, k) of component COMP: the partials of the source cells at offsets
@@ -510,8 +549,10 @@ __global__ void k_p2g(Geo g, DevPtrs P) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= g.nf) return;
   Face F = decode_face(g, f);
-  double sw, swv;
-  if (F.comp == 0)
+  double sw = 0.0, swv = 0.0;
+  if (!face_reached(g, P, F.i, F.j, F.k))
+    ;
+  else if (F.comp == 0)
     face_sums<0>(g, P, F.i, F.j, F.k, &sw, &swv);
   else if (F.comp == 1)
     face_sums<1>(g, P, F.i, F.j, F.k, &sw, &swv);
@@ -742,16 +783,22 @@ __global__ void __launch_bounds__(256) k_density(Geo g, DevPtrs P) {
 
 // ---------------------------------------------------------------- advection
 
+// 128-thread blocks, five resident per SM (at most 102 registers a thread), so that the parcels of a
+// 4 mm pour (88,856) fit in one wave of the 148 SMs.
+constexpr int ADVECT_THREADS = 128;
+
 struct Sten {
   int base, sx, sxy;
   double fx, fy, fz;
 };
 
-// solver3d.ts:339-362 for component comp (0/1/2 = u/v/w faces)
-__device__ __forceinline__ Sten face_stencil(const Geo& g, int comp, double x, double y, double z) {
+// solver3d.ts:339-362 for component comp (0/1/2 = u/v/w faces), from the point's coordinates already
+// divided by h (qx = x / h, ...): the component's offset is subtracted after the division, as the
+// reference does, so the three components and every field sampled at one point share the divisions.
+__device__ __forceinline__ Sten face_stencil_q(const Geo& g, int comp, double qx, double qy, double qz) {
   double ox = comp == 0 ? 0.0 : 0.5, oy = comp == 1 ? 0.0 : 0.5, oz = comp == 2 ? 0.0 : 0.5;
   int sx = g.nx + (comp == 0), sy = g.ny + (comp == 1), sz = g.nz + (comp == 2);
-  double gx = x / g.h - ox, gy = y / g.h - oy, gz = z / g.h - oz;
+  double gx = qx - ox, gy = qy - oy, gz = qz - oz;
   // clamp(floor(g), 0, s - 2); a NaN coordinate clamps to 0, so no index is ever formed from a NaN
   // (its weights stay NaN and the sample is NaN, as the reference's is)
   auto clampi = [](double f, int hi) { return f >= 0.0 ? (f <= (double)hi ? f : (double)hi) : 0.0; };
@@ -778,43 +825,20 @@ __device__ __forceinline__ double corner_w(const Sten& s, int c) {
   return wx * wy * wz;
 }
 
-// sample() without a valid mask (solver3d.ts:386-408)
-__device__ __forceinline__ double sample(const Geo& g, const float* field, int comp, double x, double y, double z) {
-  Sten s = face_stencil(g, comp, x, y, z);
+// sample() without a valid mask (solver3d.ts:386-408) at a point given divided by h.
+__device__ __forceinline__ double sample_q(const Geo& g, const float* field, int comp, double qx, double qy,
+                                           double qz) {
+  Sten s = face_stencil_q(g, comp, qx, qy, qz);
   double all = 0;
 #pragma unroll
   for (int c = 0; c < 8; c++) all += corner_w(s, c) * (double)field[corner(s, c)];
   return all;
 }
 
-// sample() with the valid mask (solver3d.ts:386-408)
-__device__ __forceinline__ double sample_valid(const Geo& g, const float* field, const uint8_t* valid, int comp,
-                                               double x, double y, double z) {
-  Sten s = face_stencil(g, comp, x, y, z);
-  double acc = 0, ws = 0, all = 0;
-#pragma unroll
-  for (int c = 0; c < 8; c++) {
-    int idx = corner(s, c);
-    double w = corner_w(s, c);
-    double fv = (double)field[idx];
-    all += w * fv;
-    if (valid[idx]) {
-      acc += w * fv;
-      ws += w;
-    }
-  }
-  return ws > 1e-9 ? acc / ws : all;
-}
-
-// Gradient of the trilinear interpolant of component comp at (x, y, z), unmasked corners (the 3D form
-// of C = sum_i u_i grad w_ip, src/sim/solver.ts:958-964): per axis the corner differences along it,
-// weighted by the other two axes' weights, over h.
-__device__ __forceinline__ float4 interp_gradient(const Geo& g, const float* field, int comp, double x, double y,
-                                                  double z) {
-  Sten s = face_stencil(g, comp, x, y, z);
-  double u[8];
-#pragma unroll
-  for (int c = 0; c < 8; c++) u[c] = (double)field[corner(s, c)];
+// Gradient of the trilinear interpolant of one component from its 8 corner values u (corner order of
+// corner()) over stencil s, unmasked (the 3D form of C = sum_i u_i grad w_ip, src/sim/solver.ts:958-964):
+// per axis the corner differences along it, weighted by the other two axes' weights, over h.
+__device__ __forceinline__ float4 interp_gradient(const Geo& g, const Sten& s, const double u[8]) {
   const double fx = s.fx, fy = s.fy, fz = s.fz;
   const double gx = ((1 - fy) * (1 - fz) * (u[1] - u[0]) + fy * (1 - fz) * (u[3] - u[2]) +
                      (1 - fy) * fz * (u[5] - u[4]) + fy * fz * (u[7] - u[6])) / g.h;
@@ -825,30 +849,22 @@ __device__ __forceinline__ float4 interp_gradient(const Geo& g, const float* fie
   return make_float4((float)gx, (float)gy, (float)gz, 0.f);
 }
 
-// sample() of the correction velocity (solver3d.ts:386-408 on uc, vc, wc), an FP64 face field.
-__device__ __forceinline__ double sample_corr(const Geo& g, const DevPtrs& P, int comp, double x, double y,
-                                              double z) {
-  Sten s = face_stencil(g, comp, x, y, z);
-  double all = 0;
-#pragma unroll
-  for (int c = 0; c < 8; c++) all += corner_w(s, c) * P.uc[corner(s, c)];
-  return all;
-}
-
 __device__ __forceinline__ void set_status(SimScalars* sc, int from, int to) {  // solver3d.ts:790-794
   atomicSub(&sc->counts[from], 1);
   atomicAdd(&sc->counts[to], 1);
 }
 
 // One parcel's grid-to-particle update and advection; returns the FP64 bits of its |v|^2 when it
-// stays in the pot (the stableDt input of the next substep), else 0.
+// stays in the pot (the stableDt input of the next substep), else 0. APIC is the transfer
+// (g.apic), fixed per instantiation so that the FLIP kernel does not carry the affine state.
+template <bool APIC>
 __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const DevPtrs& P, SimScalars* sc, int p) {
   float4 pos = P.pos_sorted[p];
   float4 vel = P.vel_sorted[p];
   int meta = __float_as_int(vel.w);
   int st = meta & 0xff;
   const double dt = sc->dt;
-  if (st != IN_POT && g.apic)  // a removed parcel keeps its own affine state (the slot is re-used every substep)
+  if (st != IN_POT && APIC)  // a removed parcel keeps its own affine state (the slot is re-used every substep)
 #pragma unroll
     for (int a = 0; a < 3; a++) P.aff_home[a * g.n + p] = P.aff_sorted[a * g.n + p];
   if (st == DISCHARGED || st == SPILLED) {  // solver3d.ts:693-702
@@ -870,46 +886,63 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
   }
   const double x0 = pos.x, y0 = pos.y, z0 = pos.z;
   double vx = vel.x, vy = vel.y, vz = vel.z;
-  // gridToParticles (solver3d.ts:607-624): FLIP/PIC blend with valid-masked samples; APIC: the masked
-  // PIC sample and the gradient of each component's interpolant (src/sim/solver.ts:956-986 in 3D)
-  if (g.apic) {
-    const float* U = P.u;
-    const uint8_t* V = P.valid;
-    vx = sample_valid(g, U, V, 0, x0, y0, z0);
-    vy = sample_valid(g, U, V, 1, x0, y0, z0);
-    vz = sample_valid(g, U, V, 2, x0, y0, z0);
+  // Every field sampled at the parcel's position, with one stencil per face component: gridToParticles
+  // (solver3d.ts:607-624: the FLIP/PIC blend of valid-masked samples of u and uprev; APIC: the masked
+  // sample of u and the gradient of each component's interpolant, src/sim/solver.ts:956-986 in 3D), the
+  // unmasked sample of u that starts the midpoint step and the correction velocity (solver3d.ts:704-727).
+  const bool corr = g.kappa > 0 && sc->corr_any;
+  const double qx0 = x0 / g.h, qy0 = y0 / g.h, qz0 = z0 / g.h;
+  double u1[3], cs[3], vg[3];
 #pragma unroll
-    for (int a = 0; a < 3; a++) P.aff_home[a * g.n + p] = interp_gradient(g, U, a, x0, y0, z0);
-  } else {
-    const float* U = P.u;
-    const float* UP = P.uprev;
-    const uint8_t* V = P.valid;
-    double un = sample_valid(g, U, V, 0, x0, y0, z0);
-    double vn = sample_valid(g, U, V, 1, x0, y0, z0);
-    double wn = sample_valid(g, U, V, 2, x0, y0, z0);
-    double uo = sample_valid(g, UP, V, 0, x0, y0, z0);
-    double vo = sample_valid(g, UP, V, 1, x0, y0, z0);
-    double wo = sample_valid(g, UP, V, 2, x0, y0, z0);
-    double a = g.flip;
-    vx = (1 - a) * un + a * (vx + un - uo);
-    vy = (1 - a) * vn + a * (vy + vn - vo);
-    vz = (1 - a) * wn + a * (vz + wn - wo);
+  for (int a = 0; a < 3; a++) {
+    const Sten s = face_stencil_q(g, a, qx0, qy0, qz0);
+    double fu[8];
+    double all = 0, acc = 0, ws = 0, allp = 0, accp = 0, call = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int idx = corner(s, c);
+      const double w = corner_w(s, c);
+      fu[c] = (double)P.u[idx];
+      const bool ok = P.valid[idx] != 0;
+      all += w * fu[c];
+      if (ok) {
+        acc += w * fu[c];
+        ws += w;
+      }
+      if (!APIC) {
+        const double fp = (double)P.uprev[idx];
+        allp += w * fp;
+        if (ok) accp += w * fp;
+      }
+      if (corr) call += w * P.uc[idx];
+    }
+    u1[a] = all;
+    cs[a] = call;
+    const double un = ws > 1e-9 ? acc / ws : all;
+    if (APIC) {
+      vg[a] = un;
+      P.aff_home[a * g.n + p] = interp_gradient(g, s, fu);
+    } else {
+      const double uo = ws > 1e-9 ? accp / ws : allp;
+      const double v = a == 0 ? vx : a == 1 ? vy : vz;
+      vg[a] = (1 - g.flip) * un + g.flip * (v + un - uo);
+    }
   }
+  vx = vg[0];
+  vy = vg[1];
+  vz = vg[2];
   // advect (solver3d.ts:704-787)
   double loc0[3], loc1[3], out[3];
   to_local(g, sc->c0, sc->s0, x0, y0, z0, loc0);
-  const float* U = P.u;
-  double u1 = sample(g, U, 0, x0, y0, z0);
-  double v1 = sample(g, U, 1, x0, y0, z0);
-  double w1 = sample(g, U, 2, x0, y0, z0);
-  double xm = x0 + 0.5 * dt * u1, ym = y0 + 0.5 * dt * v1, zm = z0 + 0.5 * dt * w1;
-  double x1 = x0 + dt * sample(g, U, 0, xm, ym, zm);
-  double y1 = y0 + dt * sample(g, U, 1, xm, ym, zm);
-  double z1 = z0 + dt * sample(g, U, 2, xm, ym, zm);
-  if (g.kappa > 0 && sc->corr_any) {
-    x1 += dt * sample_corr(g, P, 0, x0, y0, z0);
-    y1 += dt * sample_corr(g, P, 1, x0, y0, z0);
-    z1 += dt * sample_corr(g, P, 2, x0, y0, z0);
+  const double xm = x0 + 0.5 * dt * u1[0], ym = y0 + 0.5 * dt * u1[1], zm = z0 + 0.5 * dt * u1[2];
+  const double qxm = xm / g.h, qym = ym / g.h, qzm = zm / g.h;
+  double x1 = x0 + dt * sample_q(g, P.u, 0, qxm, qym, qzm);
+  double y1 = y0 + dt * sample_q(g, P.u, 1, qxm, qym, qzm);
+  double z1 = z0 + dt * sample_q(g, P.u, 2, qxm, qym, qzm);
+  if (corr) {
+    x1 += dt * cs[0];
+    y1 += dt * cs[1];
+    z1 += dt * cs[2];
   }
   const double c1 = sc->c1, s1 = sc->s1;
   const double margin = 0.1 * g.h, eps = 1e-4;
@@ -1000,11 +1033,12 @@ __device__ __forceinline__ unsigned long long advect_one(const Geo& g, const Dev
 
 // The maximum speed is folded per warp (bit patterns of non-negative doubles order like the values),
 // so one atomic per warp reaches the scalar block instead of one per parcel.
-__global__ void __launch_bounds__(256, 2) k_advect(Geo g, DevPtrs P) {
+template <bool APIC>
+__global__ void __launch_bounds__(ADVECT_THREADS, 5) k_advect(Geo g, DevPtrs P) {
   SimScalars* sc = P.sc;
   if (!sc->active) return;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long bits = p < g.n ? advect_one(g, P, sc, p) : 0ull;
+  unsigned long long bits = p < g.n ? advect_one<APIC>(g, P, sc, p) : 0ull;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long ob = __shfl_xor_sync(0xffffffffu, bits, o);
@@ -1056,21 +1090,14 @@ void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_bin_permute<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
 }
 
-void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st) {
-  if (g.apic)
-    k_p2g_cells<true><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
-  else
-    k_p2g_cells<false><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
-  k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
-}
-
 // The cells' node partials, then the faces (k_p2g, this stream) and the density stage (k_density,
 // the second stream) side by side: both only read the partials, and they write disjoint arrays.
 void launch_p2g_cells(const Geo& g, const DevPtrs& P, cudaStream_t st) {
+  const dim3 grid(min(blocks(g.nc, P2G_CELL_THREADS), P2G_CELL_BLOCKS), 4);
   if (g.apic)
-    k_p2g_cells<true><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+    k_p2g_cells<true><<<grid, P2G_CELL_THREADS, 0, st>>>(g, P);
   else
-    k_p2g_cells<false><<<dim3(blocks(g.nc, 128), 4), 128, 0, st>>>(g, P);
+    k_p2g_cells<false><<<grid, P2G_CELL_THREADS, 0, st>>>(g, P);
 }
 void launch_p2g_faces(const Geo& g, const DevPtrs& P, cudaStream_t st) {
   k_p2g<<<blocks(g.nf, 256), 256, 0, st>>>(g, P);
@@ -1086,7 +1113,10 @@ void launch_stage_density(const Geo& g, const DevPtrs& P, cudaStream_t st) {
 }
 
 void launch_stage_advect(const Geo& g, const DevPtrs& P, cudaStream_t st) {
-  k_advect<<<blocks(g.n, 256), 256, 0, st>>>(g, P);
+  if (g.apic)
+    k_advect<true><<<blocks(g.n, ADVECT_THREADS), ADVECT_THREADS, 0, st>>>(g, P);
+  else
+    k_advect<false><<<blocks(g.n, ADVECT_THREADS), ADVECT_THREADS, 0, st>>>(g, P);
 }
 
 void launch_render(const Geo& g, const DevPtrs& P, cudaStream_t st) {

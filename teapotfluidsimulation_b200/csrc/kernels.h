@@ -41,7 +41,6 @@ SolverWs solver_ws_carve(void* base, int cap);
 size_t solver_ws_bytes(int cap);
 
 void launch_stage_bin(const Geo& g, const DevPtrs& P, cudaStream_t st);
-void launch_stage_p2g(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_stage_extrap(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_stage_density(const Geo& g, const DevPtrs& P, cudaStream_t st);
 void launch_stage_advect(const Geo& g, const DevPtrs& P, cudaStream_t st);
