@@ -386,6 +386,8 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
   };
   const uint32_t WCNT = take(size_t(K) * CHEB_CLUSTER * (CHEB_MAX_THREADS / 32) * 4);  // per (k, rank, warp)
   const uint32_t SENDL = take(size_t(chunk) * 6 * 8);  // (own index | rank << 16, halo slot), by (rank, slot)
+  const uint32_t NBOS = take(size_t(chunk) * 6 * 4);   // neighbour offsets by position, [f][own index]
+  const uint32_t PERM = take(size_t(chunk) * 4);       // own index of each compute slot
   const uint32_t VEC0 = off;
   // per (k, rank, warp): cells of the warp's k-th group with a neighbour owned by the rank
 #pragma unroll
@@ -446,18 +448,56 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
             make_uint2(uint32_t(tid + k * nt) | (uint32_t(r) << 16), uint32_t(C.in_base[r] + idx));
       }
     }
-  // byte offsets of the own cells' neighbours in a stencil vector of T (the guard for none)
-  uint32_t nbo[K][6];
+  // byte offsets of the own cells' neighbours in a stencil vector of T (the guard for none), by position
   bool has[K];
 #pragma unroll
   for (int k = 0; k < K; k++) {
     has[k] = tid + k * nt < cnt;
+    if (has[k])
 #pragma unroll
-    for (int f = 0; f < 6; f++) {
-      const int gi = gnb[k][f];
-      const int li = gi < 0 ? guard : (gi / chunk == me ? gi - own0 : guard + 1 + hrank(gi));
-      nbo[k][f] = uint32_t(li) * uint32_t(sizeof(T));
+      for (int f = 0; f < 6; f++) {
+        const int gi = gnb[k][f];
+        const int li = gi < 0 ? guard : (gi / chunk == me ? gi - own0 : guard + 1 + hrank(gi));
+        sv<uint32_t>(smem, NBOS, f * chunk + tid + k * nt) = uint32_t(li) * uint32_t(sizeof(T));
+      }
+  }
+  // Compute slots: the boundary cells (those some rank holds in its halo) first, in position order, then
+  // the interior cells, so that a round computes whole warps of boundary cells before its send pass
+  // and the interior cells while the sends are in flight. Slot t_k = tid + k * nt computes own cell
+  // oi[k]; the cells' values and the send lists stay by position.
+  int brank[K], nbnd = 0;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const bool b = has[k] && dmask[k] != 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, b);
+    if (lane == 0) s_warp[wid] = __popc(bal);
+    __syncthreads();
+    int before = nbnd, tot = 0;
+    for (int w = 0; w < nwarps; w++) {
+      const int c = s_warp[w];
+      before += w < wid ? c : 0;
+      tot += c;
     }
+    brank[k] = before + __popc(bal & ((1u << lane) - 1u));
+    nbnd += tot;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    if (has[k]) {
+      const int t = tid + k * nt;
+      sv<int>(smem, PERM, dmask[k] != 0 ? brank[k] : nbnd + t - brank[k]) = t;
+    }
+  __syncthreads();
+  int oi[K];
+  bool bnd[K];
+  uint32_t nbo[K][6];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    oi[k] = has[k] ? sv<int>(smem, PERM, tid + k * nt) : 0;
+    bnd[k] = has[k] && tid + k * nt < nbnd;
+#pragma unroll
+    for (int f = 0; f < 6; f++) nbo[k][f] = has[k] ? sv<uint32_t>(smem, NBOS, f * chunk + oi[k]) : 0u;
   }
   __syncthreads();
   // ---- per-thread state of the owned cells (the exchange data serves every job of the launch)
@@ -466,21 +506,18 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
   int li_own[K];  // liquid-list index of each own cell
 #pragma unroll
   for (int k = 0; k < K; k++) {
-    const int t = tid + k * nt;
-    const int li = has[k] ? P.tperm[own0 + t] : 0;
+    const int li = has[k] ? P.tperm[own0 + oi[k]] : 0;
     li_own[k] = li;
     const double d = has[k] ? W.adiag[li] : 1.0;
     dg[k] = T(d);
     idg[k] = T(1) / T(d);
   }
   const uint32_t xb0 = s_addr(&C.xbar[0]);
-  // Store v (a T) as own cell t_k of the vector at byte offset voff (the round's send pass carries
-  // it to the requesting ranks).
-  auto put = [&](uint32_t voff, int k, T v) {
-    stsh<T>(smem, voff + uint32_t(tid + k * nt) * uint32_t(sizeof(T)), v);
-  };
+  // Store v (a T) as this thread's own cell k of the vector at byte offset voff (the round's send pass
+  // carries it to the requesting ranks).
+  auto put = [&](uint32_t voff, int k, T v) { stsh<T>(smem, voff + uint32_t(oi[k]) * uint32_t(sizeof(T)), v); };
   // The same for an FP64 vector (the solution q in the FP32 refinement).
-  auto put64 = [&](uint32_t voff, int k, double v) { stsh<double>(smem, voff + uint32_t(tid + k * nt) * 8u, v); };
+  auto put64 = [&](uint32_t voff, int k, double v) { stsh<double>(smem, voff + uint32_t(oi[k]) * 8u, v); };
   // End of an exchange round of the vector at byte offset voff, values of V: once every own value of
   // the round is stored, the send pass stores each requested value into its halo slot of the
   // requesting rank on that rank's barrier of this round; then warp 0 alone polls this rank's barrier
@@ -510,41 +547,58 @@ __global__ void __launch_bounds__(CHEB_MAX_THREADS / K, 1) k_chebpcg(Geo g, DevP
     const T x4 = ldsh<T>(smem, voff + nbo[k][4]), x5 = ldsh<T>(smem, voff + nbo[k][5]);
     return ((x0 + x1) + (x2 + x3)) + (x4 + x5);
   };
+  // A Chebyshev round whose output is the vector at byte offset out: cell(k) computes and stores this
+  // thread's own cell k. The boundary cells come first; one CTA barrier later the send pass stores them
+  // into the holding ranks' halos, and the interior cells are computed while those stores are in flight;
+  // then warp 0 waits for this rank's halo and a CTA barrier orders the round's reads after it.
+  auto cheb_round = [&](uint32_t out, auto&& cell) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (bnd[k]) cell(k);
+    __syncthreads();
+    const uint32_t bo = uint32_t(e & 1) * 8u;
+    for (int i = tid; i < incoming; i += nt) {
+      const uint2 en = sv<uint2>(smem, SENDL, i);
+      const int rk = int(en.x >> 16);
+      const T v = ldsh<T>(smem, out + (en.x & 0xffffu) * uint32_t(sizeof(T)));
+      st_async(C.rsmem[rk] + out + (uint32_t(guard + 1) + en.y) * uint32_t(sizeof(T)), v, C.rxbar[rk] + bo);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (has[k] && !bnd[k]) cell(k);
+    const uint32_t bar = xb0 + bo;
+    if (tid == 0) mbar_expect(bar, uint32_t(nh) * uint32_t(sizeof(T)));
+    if (tid < 32) mbar_wait(bar, uint32_t(e >> 1) & 1u, ok);
+    __syncthreads();
+    e++;
+  };
   const T itheta = T(2.0 / (2.0 + a.cheb_lo));
   // z = p(D^-1 A) D^-1 r, published (own cells and halo) in ZS
   auto precondition = [&]() {
     uint32_t out = deg > 1 ? ((e & 1) ? DV1 : DV0) : ZS;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      if (!has[k]) continue;
+    cheb_round(out, [&](int k) {
       const T d = r[k] * idg[k] * itheta;
       cdown[k] = d;
       z[k] = d;
       res[k] = r[k];
       put(out, k, d);
-    }
+    });
     uint32_t last = out;
-    round_end(out, T());
     for (int s = 1; s < deg; s++) {
       const T c1 = sizeof(T) == 4 ? T(C.coef_f[s][0]) : T(C.coef[s][0]);
       const T c2 = sizeof(T) == 4 ? T(C.coef_f[s][1]) : T(C.coef[s][1]);
-      T acc[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = has[k] ? nsum(last, k) : T(0);
       const bool final_step = s + 1 == deg;
       out = final_step ? ZS : ((e & 1) ? DV1 : DV0);
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        if (!has[k]) continue;
-        const T rs = res[k] - (dg[k] * cdown[k] - acc[k]);
+      cheb_round(out, [&](int k) {
+        const T acc = nsum(last, k);
+        const T rs = res[k] - (dg[k] * cdown[k] - acc);
         res[k] = rs;
         const T d = c1 * cdown[k] + c2 * rs * idg[k];
         cdown[k] = d;
         z[k] += d;
         put(out, k, final_step ? z[k] : d);
-      }
+      });
       last = out;
-      round_end(out, T());
     }
   };
   // w = A z from the published z; partial z.r and z.w
