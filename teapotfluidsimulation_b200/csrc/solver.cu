@@ -71,16 +71,11 @@ __global__ void k_solve_setup(Geo g, DevPtrs P, SolverWs W, int compute_rhs, int
   const bool tiled = tile_order && g.tiled;
   if (tiled) {
     const int T = g.ntx * g.nty * g.nz;
-    // the populations, read coalesced with several loads in flight per thread, then summed from
-    // shared memory over each thread's consecutive range
-#pragma unroll 4
-    for (int e = threadIdx.x; e < T; e += blockDim.x) s_pre[e] = __popcll(P.tile_mask[e]);
-    __syncthreads();
     const int per = (T + blockDim.x - 1) / blockDim.x;
     const int e0 = threadIdx.x * per;
     int sum = 0;
     for (int q = 0; q < per; q++)
-      if (e0 + q < T) sum += s_pre[e0 + q];
+      if (e0 + q < T) sum += __popcll(P.tile_mask[e0 + q]);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     int x = sum;
 #pragma unroll
@@ -102,9 +97,8 @@ __global__ void k_solve_setup(Geo g, DevPtrs P, SolverWs W, int compute_rhs, int
     int run = s_warp[wid] + x - sum;
     for (int q = 0; q < per; q++)
       if (e0 + q < T) {
-        const int c = s_pre[e0 + q];
         s_pre[e0 + q] = run;
-        run += c;
+        run += __popcll(P.tile_mask[e0 + q]);
       }
     __syncthreads();
   }
