@@ -11,7 +11,7 @@ Tolerances:
   - pressure and projected velocity after one substep, against the oracle solved to a max-norm
     relative residual of 1e-12 (the FP64 reference solution): relative L2 < 1e-5. The reference's
     own MIC(0) solve at 1e-6 sits ~5e-8 from that solution at a 4 mm mid-pour state; measured for the
-    engine: Chebyshev/MIXED 1.3e-7 (velocity 2.1e-7), box multigrid 2.9e-7, cluster multigrid 4.9e-7,
+    engine: Chebyshev/MIXED 7.9e-8 (velocity 1.6e-7), box multigrid 2.9e-7, cluster multigrid 4.9e-7,
     MIC(0) 4.8e-8, and 3.2e-7 for the 2.5 mm full-domain APIC configuration;
   - particle-to-grid velocity (no solve involved): relative L2 < 1e-5;
   - density-correction velocity: both sides solve it to the reference's fixed 1e-4 tolerance with
@@ -20,8 +20,8 @@ Tolerances:
     and tilt angle within 2e-6 relative (measured 1.7e-7 and 7.2e-7), the iteration count equal, max
     divergence within 5% (measured 3e-5) and interior density within 1e-6 (measured 3e-8). The
     Chebyshev solve stops at a different iterate inside the same 1e-6 rule, which moves the velocities
-    and so every later stable dt by ~1e-6: time and angle within 1e-5 (measured 8e-7 and 3.6e-6),
-    interior density within 5e-6 (measured 1.3e-6).
+    and so every later stable dt by ~1e-6: time and angle within 1e-5 (measured 3.3e-7 and 1.4e-6),
+    interior density within 5e-6 (measured 3.5e-6).
 """
 import numpy as np
 import pytest
