@@ -354,13 +354,31 @@ __device__ __forceinline__ void row_sum(const T* x, const uint8_t* diag, const T
 
 // ---------------------------------------------------------------- multigrid kernels
 
+// Neighbour value x[n] of fine cell n = (i, j, k) of snapshot s with the coarse correction of its
+// parent applied: x_fine + omega x_coarse(parent) where the parent is an unknown (the prolongation of
+// multigrid.ts:150-156, over-relaxed), formed where it is read.
+template <typename T>
+__device__ __forceinline__ T prolonged(const T* x, const T* xc, const uint8_t* codec, const TG& Gc, int s, int n,
+                                       int i, int j, int k) {
+  const int cc = (s << Gc.lnc) + ((k >> (Gc.rz - 1)) * Gc.ny + (j >> (Gc.ry - 1))) * Gc.nx + (i >> (Gc.rx - 1));
+  const T v = x[n];
+  return (codec[cc] & C_SELF) ? v + T(MG_OMEGA) * xc[cc] : v;
+}
+
 // One red-black half-sweep of colour `color` ((i + j + k) & 1) on a level: x = (b + sum of the
-// weighted unknown neighbours) / diagonal. first: the first half-sweep of a V-cycle from x = 0. One
-// thread per cell of the colour (128 of a tile's 256 cells), two tiles per CTA.
+// weighted unknown neighbours) / diagonal. first: the first half-sweep of a V-cycle from x = 0. The
+// neighbours are all of the other colour, and the half-sweep after this one overwrites that colour
+// without reading it, so two passes of the V-cycle are formed where this one reads them instead:
+// - xc (the coarse level's solution, its codes codec and geometry Gc): the neighbours with the coarse
+//   correction applied (the first post-smoothing half-sweep, in place of a prolongation pass);
+// - nb_from_zero: the neighbours' values after a first half-sweep from x = 0, b / diagonal (the
+//   second pre-smoothing half-sweep, in place of the first).
+// One thread per cell of the colour (128 of a tile's 256 cells), two tiles per CTA.
 template <typename T>
 __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                    const T* w, const T* dg, int cells, T* x, const T* b,
-                                                   int color, int first, const Snap* st, const int* nact) {
+                                                   int color, int first, const Snap* st, const int* nact,
+                                                   const T* xc, const uint8_t* codec, TG Gc, int nb_from_zero) {
   pdl_enter();
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
   if (ti >= *nact) return;
@@ -379,8 +397,45 @@ __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const u
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   T off = T(0), d;
-  if (first) d = w ? dg[c] : T(diag[c]);
-  else row_sum(x, diag, w, dg, cells, c, cd, G.nx, G.nx * G.ny, off, d);
+  if (first) {
+    d = w ? dg[c] : T(diag[c]);
+  } else if (nb_from_zero) {
+    const int nx = G.nx, nxy = G.nx * G.ny;
+    auto z0 = [&](int n) { return b[n] / (w ? dg[n] : T(diag[n])); };
+    const T va = (cd & 1) ? z0(c - 1) : T(0), vb = (cd & 2) ? z0(c + 1) : T(0);
+    const T ve = (cd & 4) ? z0(c - nx) : T(0), vf = (cd & 8) ? z0(c + nx) : T(0);
+    const T vg = (cd & 16) ? z0(c - nxy) : T(0), vh = (cd & 32) ? z0(c + nxy) : T(0);
+    if (w) {  // wsum's terms and order
+      const T a = (cd & 1) ? w[c] * va : T(0), bb = (cd & 2) ? w[cells + c] * vb : T(0);
+      const T e = (cd & 4) ? w[2 * cells + c] * ve : T(0), f = (cd & 8) ? w[3 * cells + c] * vf : T(0);
+      const T gg = (cd & 16) ? w[4 * cells + c] * vg : T(0), h = (cd & 32) ? w[5 * cells + c] * vh : T(0);
+      off = ((a + bb) + (e + f)) + (gg + h);
+      d = dg[c];
+    } else {  // nsum's order
+      off = ((va + vb) + (ve + vf)) + (vg + vh);
+      d = T(diag[c]);
+    }
+  } else if (xc) {
+    const int nx = G.nx, nxy = G.nx * G.ny;
+    const T va = (cd & 1) ? prolonged(x, xc, codec, Gc, s, c - 1, i - 1, j, k) : T(0);
+    const T vb = (cd & 2) ? prolonged(x, xc, codec, Gc, s, c + 1, i + 1, j, k) : T(0);
+    const T ve = (cd & 4) ? prolonged(x, xc, codec, Gc, s, c - nx, i, j - 1, k) : T(0);
+    const T vf = (cd & 8) ? prolonged(x, xc, codec, Gc, s, c + nx, i, j + 1, k) : T(0);
+    const T vg = (cd & 16) ? prolonged(x, xc, codec, Gc, s, c - nxy, i, j, k - 1) : T(0);
+    const T vh = (cd & 32) ? prolonged(x, xc, codec, Gc, s, c + nxy, i, j, k + 1) : T(0);
+    if (w) {  // wsum's terms and order
+      const T a = (cd & 1) ? w[c] * va : T(0), bb = (cd & 2) ? w[cells + c] * vb : T(0);
+      const T e = (cd & 4) ? w[2 * cells + c] * ve : T(0), f = (cd & 8) ? w[3 * cells + c] * vf : T(0);
+      const T gg = (cd & 16) ? w[4 * cells + c] * vg : T(0), h = (cd & 32) ? w[5 * cells + c] * vh : T(0);
+      off = ((a + bb) + (e + f)) + (gg + h);
+      d = dg[c];
+    } else {  // nsum's order
+      off = ((va + vb) + (ve + vf)) + (vg + vh);
+      d = T(diag[c]);
+    }
+  } else {
+    row_sum(x, diag, w, dg, cells, c, cd, G.nx, G.nx * G.ny, off, d);
+  }
   x[c] = (b[c] + off) / d;
 }
 
@@ -437,8 +492,7 @@ __global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* list
     int s, i, j, k, c;
     tile_cell(Gf, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
     if (!(codef[c] & C_SELF)) continue;
-    const int cc = (s << Gc.lnc) + ((k >> (Gc.rz - 1)) * Gc.ny + (j >> (Gc.ry - 1))) * Gc.nx + (i >> (Gc.rx - 1));
-    if (codec[cc] & C_SELF) xf[c] += T(MG_OMEGA) * xc[cc];
+    xf[c] = prolonged(xf, xc, codec, Gc, s, c, i, j, k);
   }
 }
 
@@ -1085,7 +1139,8 @@ struct PoissonT : PoissonImpl {
     for (int q = 0; q < MG_NU; q++)
       for (int color = 0; color < 2; color++)
         lk(k_mg_smooth<T>, grid2(lim(0)), PT, s0, G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
-                                                     int(count * G.nc), z, r, color, 0, st, nact_d(0));
+                                                     int(count * G.nc), z, r, color, 0, st, nact_d(0),
+                                                     (const T*)nullptr, (const uint8_t*)nullptr, G, 0);
   }
 
   void mg_or_mic0(cudaStream_t s0) {
@@ -1100,16 +1155,28 @@ struct PoissonT : PoissonImpl {
     auto X = [&](int l) { return l == 0 ? z : L[l].x; };
     auto B = [&](int l) -> const T* { return l == 0 ? r : L[l].b; };
     auto cells = [&](int l) { return (long long)count * L[l].G.nc; };
-    auto smooth = [&](int l, int color, int first) {
+    // with_coarse: the neighbours read with level l + 1's correction applied (the first post-smoothing
+    // half-sweep, in place of a prolongation pass); from_zero: the neighbours read as a first
+    // half-sweep from x = 0 leaves them (the second pre-smoothing half-sweep, in place of the first)
+    auto smooth = [&](int l, int color, int first, bool with_coarse = false, bool from_zero = false) {
       lk(k_mg_smooth<T>, grid2(lim(l)), PT, s0, L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
-                                                   cells(l), X(l), B(l), color, first, st, nact_d(l));
+                                                   cells(l), X(l), B(l), color, first, st, nact_d(l),
+                                                   with_coarse ? (const T*)L[l + 1].x : (const T*)nullptr,
+                                                   with_coarse ? (const uint8_t*)L[l + 1].code : (const uint8_t*)nullptr,
+                                                   with_coarse ? L[l + 1].G : L[l].G, from_zero ? 1 : 0);
     };
     const int top = nlev - 1;
+    static_assert(MG_NU >= 2, "the first pre-smoothing half-sweep is read on the fly by the second");
+    // The two passes are read on the fly in single-box solves only (measured): the engine's grid-scale
+    // solves (one 128 x 128 x 64 box, launch-latency bound) take 2.31 -> 2.17 ms per substep with
+    // every level fused, while the 64 x 128^3 batch only loses: 33.7 ms unfused, 35.2 with every level
+    // fused, 35.3 with its two large levels fused and 37.2 with the others.
+    auto fused = [&](int) { return count == 1; };
     for (int l = 0; l < top; l++) {
       if (!any(l)) continue;
       for (int q = 0; q < MG_NU; q++) {
-        smooth(l, 0, q == 0);
-        smooth(l, 1, 0);
+        if (q > 0 || !fused(l)) smooth(l, 0, q == 0);
+        smooth(l, 1, 0, false, q == 0 && fused(l));  // colour 0 from x = 0, read on the fly when fused
       }
       if (any(l + 1))
         lk(k_mg_restrict<T>, grid2(lim(l + 1)), PT, s0, L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
@@ -1133,11 +1200,12 @@ struct PoissonT : PoissonImpl {
     }
     for (int l = top - 1; l >= 0; l--) {
       if (!any(l)) continue;
-      if (any(l + 1))
+      const bool pro = any(l + 1);
+      if (pro && !fused(l))
         lk(k_mg_prolong<T>, grid2(lim(l)), PT, s0, L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
                                                      L[l + 1].code, L[l + 1].x, st, nact_d(l));
       for (int q = 0; q < MG_NU; q++) {
-        smooth(l, 1, 0);
+        smooth(l, 1, 0, q == 0 && pro && fused(l));  // the coarse correction read on the fly when fused
         smooth(l, 0, 0);
       }
     }
