@@ -374,11 +374,13 @@ __device__ __forceinline__ T prolonged(const T* x, const T* xc, const uint8_t* c
 // - nb_from_zero: the neighbours' values after a first half-sweep from x = 0, b / diagonal (the
 //   second pre-smoothing half-sweep, in place of the first).
 // One thread per cell of the colour (128 of a tile's 256 cells), two tiles per CTA.
-template <typename T>
+// NB selects how the neighbours are read, one instantiation each so that the plain sweep keeps its
+// own registers: 0 as stored, 1 with the coarse correction (xc), 2 as from x = 0 (nb_from_zero).
+template <typename T, int NB>
 __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const uint8_t* code, const uint8_t* diag,
                                                    const T* w, const T* dg, int cells, T* x, const T* b,
                                                    int color, int first, const Snap* st, const int* nact,
-                                                   const T* xc, const uint8_t* codec, TG Gc, int nb_from_zero) {
+                                                   const T* xc, const uint8_t* codec, TG Gc) {
   pdl_enter();
   const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
   if (ti >= *nact) return;
@@ -397,9 +399,9 @@ __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const u
   const uint8_t cd = code[c];
   if (!(cd & C_SELF)) return;
   T off = T(0), d;
-  if (first) {
+  if (NB == 0 && first) {
     d = w ? dg[c] : T(diag[c]);
-  } else if (nb_from_zero) {
+  } else if constexpr (NB == 2) {
     const int nx = G.nx, nxy = G.nx * G.ny;
     auto z0 = [&](int n) { return b[n] / (w ? dg[n] : T(diag[n])); };
     const T va = (cd & 1) ? z0(c - 1) : T(0), vb = (cd & 2) ? z0(c + 1) : T(0);
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(PT) k_mg_smooth(TG G, const int* list, const u
       off = ((va + vb) + (ve + vf)) + (vg + vh);
       d = T(diag[c]);
     }
-  } else if (xc) {
+  } else if constexpr (NB == 1) {
     const int nx = G.nx, nxy = G.nx * G.ny;
     const T va = (cd & 1) ? prolonged(x, xc, codec, Gc, s, c - 1, i - 1, j, k) : T(0);
     const T vb = (cd & 2) ? prolonged(x, xc, codec, Gc, s, c + 1, i + 1, j, k) : T(0);
@@ -474,25 +476,6 @@ __global__ void __launch_bounds__(PT) k_mg_restrict(TG Gf, TG Gc, const int* lis
       acc += bf[cf] - (d * xf[cf] - off);
     }
     bc[c] = acc;
-  }
-}
-
-// x_fine += omega x_coarse(parent) where the parent is an unknown (multigrid.ts:150-156, over-relaxed).
-// Two tiles per CTA, two cells per thread.
-template <typename T>
-__global__ void __launch_bounds__(PT) k_mg_prolong(TG Gf, TG Gc, const int* listf, const uint8_t* codef, T* xf,
-                                                    const uint8_t* codec, const T* xc, const Snap* st, const int* nact) {
-  pdl_enter();
-  const int ti = blockIdx.x * 2 + (threadIdx.x >> 7);
-  if (ti >= *nact) return;
-  const int gt = listf[ti];
-  if (st[gt >> Gf.lnt].done) return;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    int s, i, j, k, c;
-    tile_cell(Gf, gt, (threadIdx.x & 127) + q * 128, s, i, j, k, c);
-    if (!(codef[c] & C_SELF)) continue;
-    xf[c] = prolonged(xf, xc, codec, Gc, s, c, i, j, k);
   }
 }
 
@@ -1138,9 +1121,9 @@ struct PoissonT : PoissonImpl {
     // V-cycle's own post-smoothing)
     for (int q = 0; q < MG_NU; q++)
       for (int color = 0; color < 2; color++)
-        lk(k_mg_smooth<T>, grid2(lim(0)), PT, s0, G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
-                                                     int(count * G.nc), z, r, color, 0, st, nact_d(0),
-                                                     (const T*)nullptr, (const uint8_t*)nullptr, G, 0);
+        lk(k_mg_smooth<T, 0>, grid2(lim(0)), PT, s0, G, L[0].list, L[0].code, L[0].diag, L[0].w, L[0].dg,
+                                                        int(count * G.nc), z, r, color, 0, st, nact_d(0),
+                                                        (const T*)nullptr, (const uint8_t*)nullptr, G);
   }
 
   void mg_or_mic0(cudaStream_t s0) {
@@ -1159,24 +1142,18 @@ struct PoissonT : PoissonImpl {
     // half-sweep, in place of a prolongation pass); from_zero: the neighbours read as a first
     // half-sweep from x = 0 leaves them (the second pre-smoothing half-sweep, in place of the first)
     auto smooth = [&](int l, int color, int first, bool with_coarse = false, bool from_zero = false) {
-      lk(k_mg_smooth<T>, grid2(lim(l)), PT, s0, L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg,
-                                                   cells(l), X(l), B(l), color, first, st, nact_d(l),
-                                                   with_coarse ? (const T*)L[l + 1].x : (const T*)nullptr,
-                                                   with_coarse ? (const uint8_t*)L[l + 1].code : (const uint8_t*)nullptr,
-                                                   with_coarse ? L[l + 1].G : L[l].G, from_zero ? 1 : 0);
+      auto kern = with_coarse ? k_mg_smooth<T, 1> : from_zero ? k_mg_smooth<T, 2> : k_mg_smooth<T, 0>;
+      lk(kern, grid2(lim(l)), PT, s0, L[l].G, L[l].list, L[l].code, L[l].diag, L[l].w, L[l].dg, cells(l), X(l),
+         B(l), color, first, st, nact_d(l), with_coarse ? (const T*)L[l + 1].x : (const T*)nullptr,
+         with_coarse ? (const uint8_t*)L[l + 1].code : (const uint8_t*)nullptr, with_coarse ? L[l + 1].G : L[l].G);
     };
     const int top = nlev - 1;
     static_assert(MG_NU >= 2, "the first pre-smoothing half-sweep is read on the fly by the second");
-    // The two passes are read on the fly in single-box solves only (measured): the engine's grid-scale
-    // solves (one 128 x 128 x 64 box, launch-latency bound) take 2.31 -> 2.17 ms per substep with
-    // every level fused, while the 64 x 128^3 batch only loses: 33.7 ms unfused, 35.2 with every level
-    // fused, 35.3 with its two large levels fused and 37.2 with the others.
-    auto fused = [&](int) { return count == 1; };
     for (int l = 0; l < top; l++) {
       if (!any(l)) continue;
       for (int q = 0; q < MG_NU; q++) {
-        if (q > 0 || !fused(l)) smooth(l, 0, q == 0);
-        smooth(l, 1, 0, false, q == 0 && fused(l));  // colour 0 from x = 0, read on the fly when fused
+        if (q > 0) smooth(l, 0, 0);
+        smooth(l, 1, 0, false, q == 0);  // q == 0: colour 0 from x = 0, read on the fly
       }
       if (any(l + 1))
         lk(k_mg_restrict<T>, grid2(lim(l + 1)), PT, s0, L[l].G, L[l + 1].G, L[l + 1].list, L[l].code, L[l].diag,
@@ -1200,12 +1177,8 @@ struct PoissonT : PoissonImpl {
     }
     for (int l = top - 1; l >= 0; l--) {
       if (!any(l)) continue;
-      const bool pro = any(l + 1);
-      if (pro && !fused(l))
-        lk(k_mg_prolong<T>, grid2(lim(l)), PT, s0, L[l].G, L[l + 1].G, L[l].list, L[l].code, X(l),
-                                                     L[l + 1].code, L[l + 1].x, st, nact_d(l));
       for (int q = 0; q < MG_NU; q++) {
-        smooth(l, 1, 0, q == 0 && pro && fused(l));  // the coarse correction read on the fly when fused
+        smooth(l, 1, 0, q == 0 && any(l + 1));  // q == 0: the coarse correction read on the fly
         smooth(l, 0, 0);
       }
     }
