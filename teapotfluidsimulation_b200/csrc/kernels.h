@@ -5,10 +5,10 @@
 
 namespace pl {
 
-// 512 threads x 4 bins (the same 2048-bin tile as 256 x 8, shorter per-thread chains): 4 mm whole pour
-// 0.2839 -> 0.2808 ms per substep
-constexpr int SCAN_THREADS = 512;
-constexpr int SCAN_ITEMS = 4;
+// 1024 threads x 2 bins (the same 2048-bin tile as 256 x 8, shorter per-thread chains): 4 mm whole pour
+// 0.2839 ms per substep at 256 x 8, 0.2808 at 512 x 4, 0.2800 -> 0.2787 at 1024 x 2
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 2;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int SCAN_MAX_TILES = 4096;  // bins <= 8M
 constexpr int DENSITY_BLOCKS = 148;
